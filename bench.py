@@ -1,0 +1,347 @@
+"""Benchmark: Barnes-Hut body-steps/s on the seeded colliding-disks workload.
+
+Workload (default): N = 800,000 bodies, two colliding exponential disks,
+theta = 0.5, Plummer eps = 1e-3, dt = 5e-5, leapfrog, 32-bit Morton keys over
+the bounding box.  One "step" = one full pipeline pass (kick-drift, Morton,
+sort, build + fill, walk + kick) over all bodies.
+
+Own arm (default):
+  value      body-steps/s with the state resident in HBM, K steps timed with
+             CUDA events on the engine's stream; L2 (126 MB) is flushed
+             between timed steps (flush outside the timed events).
+  e2e        the same metric through the public API with host buffers: per
+             step upload(mass, pos, vel) from page-locked memory, one step,
+             download(pos, vel) into page-locked memory.
+  roofline   the dominant kernel (walk), from per-stage CUDA events recorded
+             in the step graph during the timed steps.
+  cpu_baseline  the oracle (C restatement, OpenMP, all host threads) on a
+             bounded sample of the same workload.
+Reference arm (--impl reference): the reference's algorithm on the host
+cores (the oracle port; the reference itself is WGSL and needs a WebGPU
+device, which this machine lacks).
+
+Multi-GPU (torchrun): every rank simulates its own independently seeded copy
+of the workload (weak scaling, no collective on the data path); the timed
+region is bracketed by barriers and the max over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PKG = "webgpu-fluid-sim_b200"
+DEFAULT_WORKLOAD = "colliding-disks-800k"
+FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="own", choices=["own", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- helpers
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_pkg():
+    return importlib.import_module(PKG)
+
+
+def force_error_vs_fp64(acc, mass, pos, cfg, nsample=256, seed=0):
+    """Median / p99 relative force error against an FP64 direct sum (numpy)."""
+    rng = np.random.default_rng(seed)
+    n = mass.size
+    idx = rng.choice(n, size=min(nsample, n), replace=False)
+    P = pos.astype(np.float64)
+    M = mass.astype(np.float64)
+    eps2 = float(cfg.plummerEps) ** 2
+    errs = []
+    for i in idx:
+        r = P - P[i]
+        d2 = (r * r).sum(1) + eps2
+        inv3 = d2 ** -1.5
+        inv3[i] = 0.0
+        a = cfg.gravConstant * (M * inv3) @ r
+        errs.append(np.linalg.norm(acc[i] - a) / max(np.linalg.norm(a), 1e-300))
+    errs = np.array(errs)
+    return float(np.median(errs)), float(np.percentile(errs, 99)), int(idx.size)
+
+
+def cpu_baseline(pkg, wl, seconds_budget=20.0):
+    """The oracle (C restatement, OpenMP) on a bounded sample of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    cfg = wl["config"]
+    n = wl["n"]
+    mass, pos, vel, _ = pkg.generate_scenario(wl["scenario"], n, 1, cfg.gravConstant)
+    st = orc.State(orc.params_from_config(cfg), mass, pos, vel)
+    threads = orc.load().orc_max_threads()
+    st.step(1)  # first step includes the initial force evaluation of the leapfrog
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        st.step(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > seconds_budget or steps >= 50:
+            break
+    return {"value": n * steps / el, "unit": "body-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} steps of the full {n}-body workload after 1 warm-up step "
+                      f"(oracle: reference per-body monopole walk, {threads} OpenMP threads)"}
+
+
+# ---------------------------------------------------------------- reference arm
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    pkg = load_pkg()
+    wl = pkg.WORKLOADS[args.workload]
+    # Each step is a bounded sample: the full workload for one step.
+    budget = max(10.0, 120.0 / max(args.steps + args.warmup, 1))
+    cb = cpu_baseline(pkg, wl, seconds_budget=budget)
+    line = {"impl": "reference", "metric": "body-steps/s", "value": cb["value"],
+            "unit": "body-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG32)",
+            "config": {"workload": args.workload, "bodies": wl["n"]},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "body-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- own arm
+
+def run_own(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    pkg = load_pkg()
+    wl = pkg.WORKLOADS[args.workload]
+    cfg = wl["config"]
+    n = wl["n"]
+    sim = pkg.Simulation(cfg, device=local)
+    sim.setNumBodies(n)
+    sim.setScenario(wl["scenario"], 1 + rank)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ext = torch.cuda.ExternalStream(sim.getBuffers().stream, device=dev)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # Warm-up also instantiates the profiled step graph used in the timed region.
+    sim.profile_begin(max(args.warmup, 1))
+    for _ in range(args.warmup):
+        sim.step(1)
+    sim.sync()
+    sim.profile_end()
+
+    # ---- timed region: K steps, per-step events on the engine stream ----
+    K = args.steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    sim.profile_begin(K)
+    t_wall = time.perf_counter()
+    with torch.cuda.stream(ext):
+        for i in range(K):
+            flush.zero_()                  # L2 flush, outside the timed events
+            starts[i].record(ext)
+            sim.step(1)
+            ends[i].record(ext)
+    sim.sync()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall
+    barrier()
+    clk = clocks.stop()
+    stage_ms, recorded = sim.profile_end()
+    step_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms_max = float(t.item())
+    value = world * n * K / (step_ms_max / 1e3)
+
+    # ---- walk statistics + force error (untimed) ----
+    visits, interactions = sim.walk_stats()
+    mass, pos, vel = sim.download()
+    acc = sim.read_buffer("acc", np.float32, 2 * n).reshape(n, 2)
+    med_err, p99_err, nsamp = force_error_vs_fp64(acc, mass, pos, cfg)
+
+    # ---- e2e through the public API with host buffers ----
+    E = args.e2e_steps
+    h_mass = torch.from_numpy(mass).pin_memory()
+    h_pos = torch.from_numpy(pos).pin_memory()
+    h_vel = torch.from_numpy(vel).pin_memory()
+    o_pos = torch.empty_like(h_pos).pin_memory()
+    o_vel = torch.empty_like(h_vel).pin_memory()
+    sim.upload(h_mass, h_pos, h_vel)
+    sim.step(1)
+    sim.download_into(None, o_pos, o_vel)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for _ in range(E):
+        sim.upload(h_mass, h_pos, h_vel)
+        sim.step(1)
+        sim.download_into(None, o_pos, o_vel)  # synchronises the stream
+    e1.record(ext)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * E / (float(t.item()) / 1e3)
+
+    out = None
+    if rank == 0:
+        import ctypes  # noqa: F401
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except OSError:
+            pass
+        # dominant kernel: the walk.  Algorithmic flops per launch = 16 FP32
+        # flops per interaction (monopole walk) x interactions of the step.
+        walk_ms = stage_ms["walk"] / max(recorded, 1)
+        flops = 16.0 * interactions
+        sm_mhz = clk.get("sm_max_mhz") or 1965.0
+        fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # nominal FMA peak at max clock
+        achieved = flops / (walk_ms / 1e3) / 1e12
+        roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                    "frac": achieved / fp32_peak, "traffic": None,
+                    "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2 x max SM clock);"
+                                   " no measured FP32 peak exists for this pool",
+                    "kernel": "walk", "kernel_ms": walk_ms, "interactions_per_step": interactions,
+                    "node_visits_per_step": visits}
+        stages = {k: v / max(recorded, 1) for k, v in stage_ms.items()}
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        kps = sim.kernels_per_step()
+        cb = None
+        if not args.no_cpu_baseline:
+            cb = cpu_baseline(pkg, wl)
+        out = {
+            "metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world,
+            "steps": K, "warmup": args.warmup, "ms_per_step": step_ms_max / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded PCG32 colliding exponential disks)",
+            "config": {"workload": args.workload, "bodies": n, "theta": cfg.bhTheta,
+                       "softening": f"plummer {cfg.plummerEps}", "dt": cfg.deltaTime,
+                       "integrator": cfg.integrator, "morton_bits": cfg.mortonBits,
+                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": "flushed between timed steps (256 MB write, outside the events)"},
+            "roofline": roofline,
+            "stages_ms": stages,
+            "hbm_peak_gbs": hbm,
+            "force_error_vs_fp64": {"median": med_err, "p99": p99_err, "sample": nsamp},
+            "cpu_baseline": cb,
+            "e2e": {"value": e2e_value, "unit": "body-steps/s", "h2d_bytes_per_step": 20 * n,
+                    "d2h_bytes_per_step": 16 * n, "steps": E},
+            "gpu_launches": kps * K,
+            "clocks": clk,
+            "wall_s_timed_region": wall,
+        }
+        print(json.dumps(out))
+    sim.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_own(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

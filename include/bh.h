@@ -1,0 +1,195 @@
+/*
+ * bh.h -- C ABI of the B200 Barnes-Hut engine (libbh_b200.so).
+ *
+ * This is the drop-in boundary for the per-step compute pipeline of the
+ * reference simulator (ElliottF05/webgpu-fluid-sim, class Simulation in
+ * src/simulation.ts:39-433).  Every entry point below names the reference
+ * member it replaces.  A host binding (Node-API addon, ctypes, cffi) wraps
+ * these one to one.
+ *
+ * Conventions
+ *  - Every function returns an int status: BH_OK (0) or a BH_ERR_* code.
+ *    bh_last_error(sim) returns the message of the last failure on that
+ *    handle (bh_global_last_error() for failures without a handle).
+ *  - The handle owns every device buffer.  bh_set_num_bodies/bh_set_scenario
+ *    reallocate them, exactly like simulation.ts:367-369, so device pointers
+ *    returned by bh_get_buffers stay valid only until the next set call or
+ *    bh_destroy (simulation.ts:427-429, interaction.ts:28-36).
+ *  - One CUDA stream per handle.  Work is stream-ordered and asynchronous
+ *    (like queue.submit); bh_sync waits for it.  A handle is not thread-safe;
+ *    different handles may be used from different threads.
+ *  - Host pointers are plain float arrays: mass[n], pos[2n] (x,y interleaved,
+ *    vec2<f32> as in simulation.ts:82-84), vel[2n].
+ */
+#ifndef BH_B200_H
+#define BH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define BH_OK 0
+#define BH_ERR_INVALID_ARGUMENT 1
+#define BH_ERR_CUDA 2
+#define BH_ERR_OUT_OF_MEMORY 3
+#define BH_ERR_UNKNOWN_SCENARIO 4 /* simulation.ts:363-365 throws "Unknown scenario" */
+#define BH_ERR_DEVICE_CHECK 5     /* a device-side check tripped (bounded spin, stack) */
+#define BH_ERR_NO_DEVICE 6
+#define BH_ERR_NOT_SUPPORTED 7
+
+/* ---- configuration ----------------------------------------------------- */
+#define BH_SOFTENING_REFERENCE 0 /* eps = epsMult*sqrt(G*max(m1,m2)*dt), barnes_hut.wgsl:90-91 */
+#define BH_SOFTENING_PLUMMER 1   /* constant Plummer eps (extension) */
+
+#define BH_DOMAIN_FIXED2000 0 /* square [-1000,1000)^2, lbvh.wgsl:49-57 */
+#define BH_DOMAIN_BBOX 1      /* tight bounding box of the bodies (extension) */
+
+#define BH_INTEGRATOR_SYMPLECTIC_EULER 0 /* kick then drift, barnes_hut.wgsl:110,119-120 */
+#define BH_INTEGRATOR_LEAPFROG_KDK 1     /* kick-drift-kick with cached force (extension) */
+
+/* Mirrors Config of src/config.ts:1-7 plus the engine's extensions. */
+typedef struct bh_config {
+    float grav_constant;      /* gravConstant (config.ts:10) */
+    float bh_theta;           /* bhTheta (config.ts:11) */
+    int32_t substeps;         /* substeps (config.ts:12): steps per bh_step frame */
+    float delta_time;         /* deltaTime (config.ts:13) */
+    float epsilon_multiplier; /* epsilonMultiplier (config.ts:14) */
+    int32_t softening;        /* BH_SOFTENING_* */
+    float plummer_eps;        /* used with BH_SOFTENING_PLUMMER */
+    int32_t morton_bits;      /* 32 (reference, 16 bits/axis) or 64 (32 bits/axis) */
+    int32_t morton_domain;    /* BH_DOMAIN_* for 32-bit keys; 64-bit keys use a power-of-two box */
+    int32_t integrator;       /* BH_INTEGRATOR_* */
+    int32_t leaf_size;        /* 1 = reference walk; >1: subtrees of <= leaf_size bodies are summed directly */
+    int32_t walk_block;       /* threads per walk block (0 = autotuned default) */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t use_graphs;       /* 1 = replay each step from a captured CUDA graph */
+    int32_t fp64_levels;      /* 1 = FP64 mass/COM aggregation for nodes of >= 1024 bodies */
+    int32_t reserved[7];
+} bh_config;
+
+/* getDefaultConfig() (config.ts:9-22) plus extension defaults that keep the
+ * reference behaviour (reference softening, fixed domain, 32-bit keys,
+ * symplectic Euler, leaf_size 1). */
+int bh_default_config(bh_config* out);
+
+/* ---- lifetime ----------------------------------------------------------- */
+typedef struct bh_sim bh_sim;
+
+/* new Simulation(config, device) (simulation.ts:55-66): 50000 bodies,
+ * scenario "default", buffers allocated but not yet filled. */
+int bh_create(const bh_config* config, bh_sim** out);
+int bh_destroy(bh_sim* sim);
+
+/* setNumBodies(n) (simulation.ts:227-231): reallocates and regenerates the
+ * current scenario. */
+int bh_set_num_bodies(bh_sim* sim, uint32_t n);
+
+/* setScenario(name) (simulation.ts:233-374).  Names: "default",
+ * "two-clusters", "planetary-disk" (the reference's three), and the seeded
+ * benchmark generators "uniform-disk-kepler", "colliding-disks",
+ * "gaussian-mixture", "plummer-projection".  The reference draws from
+ * Math.random(); here every draw comes from PCG32 seeded by `seed`.  Unknown
+ * names return BH_ERR_UNKNOWN_SCENARIO ("Unknown scenario: <name>"). */
+int bh_set_scenario(bh_sim* sim, const char* name, uint64_t seed);
+
+/* updateMetadataBuffer() (simulation.ts:212-225).  The engine's fill is
+ * race-free, so the random leaf offset of lbvh.wgsl:171 has no effect; this
+ * call only re-validates the configuration.  Kept for API parity. */
+int bh_update_metadata(bh_sim* sim);
+
+/* Host state in/out (queue.writeBuffer at simulation.ts:376-384, and the
+ * checkpoint path).  n must equal the body count.  Any pointer may be NULL
+ * to skip that array.  Both are asynchronous on the handle's stream for
+ * page-locked host memory; bh_download synchronises before returning. */
+int bh_upload(bh_sim* sim, const float* mass, const float* pos, const float* vel, uint32_t n);
+int bh_download(bh_sim* sim, float* mass, float* pos, float* vel, uint32_t n);
+
+/* getCommands() + queue.submit (simulation.ts:386-425, main.ts:38-41):
+ * enqueue `frames` frames of config.substeps steps each.  Asynchronous. */
+int bh_step(bh_sim* sim, uint32_t frames);
+int bh_sync(bh_sim* sim);
+
+/* Accelerations at the current positions without integrating: builds the
+ * tree and runs the walk; acc[2n] (device buffer, original body order) is
+ * copied to acc_host when it is not NULL. */
+int bh_compute_accelerations(bh_sim* sim, float* acc_host);
+
+/* ---- buffers (getBuffers(), simulation.ts:8-18,427-429) ----------------- */
+/* Device pointers borrowed from the handle.  Layouts:
+ *   mass[n], pos[2n], vel[2n], radius_multiplier[n], acc[2n]  (original body order)
+ *   morton_codes[n]: uint32 (32-bit keys) or uint64 (64-bit keys), sorted
+ *   body_indices[n]: sorted permutation (sorted slot -> body)
+ *   node4[2n-1]: float4 {com.x, com.y, mass, length}; internal nodes
+ *                [0, n-2], leaves [n-1, 2n-2] (lbvh.wgsl:94)
+ *   node_children[2(n-1)]: {left, right} per internal node
+ *   node_parent[2n-1]: parent index, 0xFFFFFFFF at the root
+ *   node_aabb[4(n-1)]: {min.x, min.y, max.x, max.y} per internal node
+ *                      (a leaf's box is its body position) */
+typedef struct bh_buffers {
+    float* mass;
+    float* pos;
+    float* vel;
+    float* radius_multiplier;
+    float* acc;
+    void* morton_codes;
+    uint32_t* body_indices;
+    float* node4;
+    uint32_t* node_children;
+    uint32_t* node_parent;
+    float* node_aabb;
+    uint32_t num_bodies;
+    int32_t morton_bits;
+    void* stream; /* cudaStream_t of the handle */
+} bh_buffers;
+
+int bh_get_buffers(bh_sim* sim, bh_buffers* out);
+int bh_get_num_bodies(bh_sim* sim, uint32_t* out); /* getNumBodies() (simulation.ts:430-432) */
+
+/* Copy `bytes` from the start of a named device buffer to host memory
+ * (synchronous).  Names: "mass", "pos", "vel", "acc", "radius_multiplier",
+ * "morton_codes", "body_indices", "node4", "node_children", "node_parent",
+ * "node_aabb". */
+int bh_read_buffer(bh_sim* sim, const char* name, void* host, size_t bytes);
+
+/* ---- host-side scenario generation (no device work) --------------------- */
+/* Fills mass[n], pos[2n], vel[2n] and (optionally) radius_multiplier[n] with
+ * the named scenario, exactly as bh_set_scenario does before its upload. */
+int bh_generate_scenario(const char* name, uint32_t n, uint64_t seed, float grav_constant,
+                         float* mass, float* pos, float* vel, float* radius_multiplier);
+
+/* ---- profiling ---------------------------------------------------------- */
+#define BH_STAGE_MORTON 0  /* bbox + Morton encode + digit histograms */
+#define BH_STAGE_SORT 1    /* radix sort passes */
+#define BH_STAGE_TREE 2    /* hierarchy build + mass/COM fill */
+#define BH_STAGE_WALK 3    /* walk + integrate */
+#define BH_STAGE_OTHER 4   /* kick-drift (leapfrog), memsets */
+#define BH_NUM_STAGES 5
+
+/* Start recording CUDA events around every stage of the next `max_steps`
+ * steps (on the handle's stream).  bh_profile_end synchronises and returns
+ * the summed milliseconds per stage and the number of steps recorded. */
+int bh_profile_begin(bh_sim* sim, uint32_t max_steps);
+int bh_profile_end(bh_sim* sim, double* stage_ms, uint32_t* steps_recorded);
+
+/* Kernels one step launches (for launch accounting). */
+int bh_kernels_per_step(bh_sim* sim, uint32_t* out);
+
+/* Build the tree at the current positions and run an instrumented force walk
+ * that counts, over all bodies, the nodes each body's walk visits and the
+ * interactions it evaluates (for rooflines).  Leaves acc[] holding the
+ * forces; does not integrate. */
+int bh_walk_stats(bh_sim* sim, uint64_t* node_visits, uint64_t* interactions);
+
+/* ---- errors ------------------------------------------------------------- */
+const char* bh_last_error(bh_sim* sim);
+const char* bh_global_last_error(void);
+const char* bh_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

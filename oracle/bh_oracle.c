@@ -1,0 +1,596 @@
+/*
+ * bh_oracle.c -- CPU restatement of the reference Barnes-Hut step pipeline.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker and the timed CPU baseline).  The CUDA
+ * engine never links or calls this file.  Each function names the reference
+ * file:line it restates.  Compile with -ffp-contract=off so that every f32
+ * operation rounds exactly as written, like the WGSL source.
+ *
+ * Parallelism: every stage is a parallel-for over the shader's invocations
+ * (OpenMP).  The results do not depend on the thread count: the sort is a
+ * stable LSD radix sort, the build is per-node independent, the fill combines
+ * the two finished children whichever arrives second (acq_rel arrival
+ * counters), and the walk is per-body independent.
+ */
+#include "bh_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define STACK_SIZE 256 /* barnes_hut.wgsl:67 */
+
+static int nthreads(const orc_params* p) {
+#ifdef _OPENMP
+    return (p && p->threads > 0) ? p->threads : omp_get_max_threads();
+#else
+    (void)p;
+    return 1;
+#endif
+}
+
+int orc_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+static inline int clz32(uint32_t x) { return x ? __builtin_clz(x) : 32; }
+static inline int clz64(uint64_t x) { return x ? __builtin_clzll(x) : 64; }
+
+/* ------------------------------------------------------------------------ */
+/* Morton encode                                                             */
+/* ------------------------------------------------------------------------ */
+
+static inline uint32_t spread16(uint32_t v) { /* bit b -> bit 2b (lbvh.wgsl:59-65) */
+    v &= 0xFFFFu;
+    v = (v | (v << 8)) & 0x00FF00FFu;
+    v = (v | (v << 4)) & 0x0F0F0F0Fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+static inline uint64_t spread32(uint64_t v) {
+    v &= 0xFFFFFFFFull;
+    v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
+    v = (v | (v << 8)) & 0x00FF00FF00FF00FFull;
+    v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0Full;
+    v = (v | (v << 2)) & 0x3333333333333333ull;
+    v = (v | (v << 1)) & 0x5555555555555555ull;
+    return v;
+}
+
+/* WGSL u32(f32) for a finite value in [0, 2^32): truncation. */
+static inline uint32_t quant16(float u) {
+    /* lbvh.wgsl:54-57: clamp to [0,1], u32(u*65535+0.5), min with 65535 */
+    if (!(u > 0.0f)) u = 0.0f; /* clamp low (NaN maps to 0) */
+    if (u > 1.0f) u = 1.0f;
+    float t = u * 65535.0f;
+    t = t + 0.5f;
+    uint32_t q = (uint32_t)t;
+    return q > 65535u ? 65535u : q;
+}
+
+void orc_domain_compute(const orc_params* p, uint32_t n, const float* pos, orc_domain* out) {
+    out->lo_x = -1000.0f; /* lbvh.wgsl:49-50: fixed square of side 2000 centred at 0 */
+    out->lo_y = -1000.0f;
+    out->extent = 2000.0f;
+    out->pow2_exp = 1;
+    float lx = INFINITY, ly = INFINITY, hx = -INFINITY, hy = -INFINITY;
+    for (uint32_t i = 0; i < n; ++i) {
+        float x = pos[2 * i], y = pos[2 * i + 1];
+        lx = fminf(lx, x); hx = fmaxf(hx, x);
+        ly = fminf(ly, y); hy = fmaxf(hy, y);
+    }
+    if (n == 0) { lx = ly = hx = hy = 0.0f; }
+    if (p->morton_bits == 64) {
+        float m = fmaxf(fmaxf(fabsf(lx), fabsf(hx)), fmaxf(fabsf(ly), fabsf(hy)));
+        int e;
+        if (m < 0x1p-60f) e = -60;
+        else { int ex; frexpf(m, &ex); e = ex + 1; } /* m < 2^ex  ->  m < 2^(e-1) */
+        out->pow2_exp = e;
+        return;
+    }
+    if (p->morton_domain == ORC_DOMAIN_BBOX) {
+        float ext = fmaxf(hx - lx, hy - ly);
+        if (!(ext > 0.0f)) ext = 1.0f;
+        out->lo_x = lx;
+        out->lo_y = ly;
+        out->extent = ext;
+    }
+}
+
+void orc_morton(const orc_params* p, const orc_domain* dom, uint32_t n, const float* pos,
+                uint64_t* codes, uint32_t* ids) {
+    int nt = nthreads(p);
+    if (p->morton_bits == 64) {
+        /* Extension: 32 bits per axis over [-2^(e-1), 2^(e-1)): q = floor(x*2^(32-e)) + 2^31,
+         * exact because scaling by a power of two is exact. */
+        float s = ldexpf(1.0f, 32 - dom->pow2_exp);
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t i = 0; i < (int64_t)n; ++i) {
+            float xs = pos[2 * i] * s, ys = pos[2 * i + 1] * s;
+            int64_t qx = (int64_t)floorf(xs) + 2147483648LL;
+            int64_t qy = (int64_t)floorf(ys) + 2147483648LL;
+            if (qx < 0) qx = 0;
+            if (qx > 4294967295LL) qx = 4294967295LL;
+            if (qy < 0) qy = 0;
+            if (qy > 4294967295LL) qy = 4294967295LL;
+            codes[i] = spread32((uint64_t)qx) | (spread32((uint64_t)qy) << 1);
+            ids[i] = (uint32_t)i;
+        }
+        return;
+    }
+    /* lbvh.wgsl:49-68 with (lo, extent) = (-1000, 2000) in the reference domain. */
+    const float lo_x = dom->lo_x, lo_y = dom->lo_y, ext = dom->extent;
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        float ux = (pos[2 * i] - lo_x) / ext;
+        float uy = (pos[2 * i + 1] - lo_y) / ext;
+        uint32_t x = quant16(ux), y = quant16(uy);
+        codes[i] = (uint64_t)(spread16(x) | (spread16(y) << 1));
+        ids[i] = (uint32_t)i; /* lbvh.wgsl:68 */
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Stable LSD radix sort (the contract of webgpu-radix-sort)                 */
+/* ------------------------------------------------------------------------ */
+
+static void radix_sort_impl(uint32_t n, uint64_t* codes, uint32_t* ids, int bits, int nt) {
+    if (n < 2) return;
+    uint64_t* kt = (uint64_t*)malloc(sizeof(uint64_t) * n);
+    uint32_t* vt = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint64_t *ks = codes, *kd = kt;
+    uint32_t *vs = ids, *vd = vt;
+    size_t* hist = (size_t*)malloc(sizeof(size_t) * 256 * (size_t)nt);
+    int passes = bits / 8;
+    for (int pass = 0; pass < passes; ++pass) {
+        int shift = 8 * pass;
+        memset(hist, 0, sizeof(size_t) * 256 * (size_t)nt);
+#pragma omp parallel num_threads(nt)
+        {
+            int t = 0, T = 1;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+            T = omp_get_num_threads();
+#endif
+            size_t lo = (size_t)n * t / T, hi = (size_t)n * (t + 1) / T;
+            size_t* h = hist + 256 * (size_t)t;
+            for (size_t i = lo; i < hi; ++i) h[(ks[i] >> shift) & 0xFF]++;
+#pragma omp barrier
+#pragma omp single
+            {
+                size_t run = 0;
+                for (int d = 0; d < 256; ++d)
+                    for (int tt = 0; tt < T; ++tt) {
+                        size_t c = hist[256 * (size_t)tt + d];
+                        hist[256 * (size_t)tt + d] = run;
+                        run += c;
+                    }
+            }
+            for (size_t i = lo; i < hi; ++i) {
+                size_t dst = h[(ks[i] >> shift) & 0xFF]++;
+                kd[dst] = ks[i];
+                vd[dst] = vs[i];
+            }
+        }
+        uint64_t* tk = ks; ks = kd; kd = tk;
+        uint32_t* tv = vs; vs = vd; vd = tv;
+    }
+    if (ks != codes) {
+        memcpy(codes, ks, sizeof(uint64_t) * n);
+        memcpy(ids, vs, sizeof(uint32_t) * n);
+    }
+    free(hist);
+    free(kt);
+    free(vt);
+}
+
+void orc_sort(uint32_t n, uint64_t* codes, uint32_t* ids) {
+    uint64_t any = 0;
+    for (uint32_t i = 0; i < n; ++i) any |= codes[i];
+    radix_sort_impl(n, codes, ids, (any >> 32) ? 64 : 32, orc_max_threads());
+}
+
+/* ------------------------------------------------------------------------ */
+/* Karras build: lbvh.wgsl:72-165                                            */
+/* ------------------------------------------------------------------------ */
+
+static inline int delta_fn(const uint64_t* k, int64_t n, int bits, int64_t i, int64_t j) {
+    /* lbvh.wgsl:72-83 (tie-break offset = key width; 64 for 64-bit keys) */
+    if (j < 0 || j >= n) return -1;
+    uint64_t a = k[i], b = k[j];
+    if (a == b) return bits + clz32((uint32_t)i ^ (uint32_t)j);
+    return bits == 64 ? clz64(a ^ b) : clz32((uint32_t)(a ^ b));
+}
+
+void orc_build(uint32_t n, int morton_bits, const uint64_t* k, uint32_t* left, uint32_t* right,
+               uint32_t* parent) {
+    if (n == 0) return;
+    const int64_t N = n;
+    const int bits = morton_bits;
+    parent[0] = 0xFFFFFFFFu; /* lbvh.wgsl:159-161; for n == 1 the root is the only leaf */
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < N - 1; ++i) {
+        int d = delta_fn(k, N, bits, i, i + 1) > delta_fn(k, N, bits, i, i - 1) ? 1 : -1;
+        int dmin = delta_fn(k, N, bits, i, i - d);
+        int64_t lmax = 2;
+        while (delta_fn(k, N, bits, i, i + d * lmax) > dmin) lmax *= 2;
+        int64_t l = 0;
+        for (int64_t t = lmax / 2; t >= 1; t /= 2)
+            if (delta_fn(k, N, bits, i, i + d * (l + t)) > dmin) l += t;
+        int64_t j = i + d * l;
+        int dnode = delta_fn(k, N, bits, i, j);
+        int64_t s = 0, t = (l + 1) / 2;
+        for (;;) {
+            if (delta_fn(k, N, bits, i, i + d * (s + t)) > dnode) s += t;
+            if (t == 1) break;
+            t = (t + 1) / 2;
+        }
+        int64_t gamma = i + d * s + (d < 0 ? d : 0);
+        int64_t mn = i < j ? i : j, mx = i < j ? j : i;
+        uint32_t lc = (mn == gamma) ? (uint32_t)(N - 1 + gamma) : (uint32_t)gamma;
+        uint32_t rc = (mx == gamma + 1) ? (uint32_t)(N - 1 + gamma + 1) : (uint32_t)(gamma + 1);
+        left[i] = lc;
+        right[i] = rc;
+        parent[lc] = (uint32_t)i;
+        parent[rc] = (uint32_t)i;
+    }
+    if (n > 1) parent[0] = 0xFFFFFFFFu;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Bottom-up fill: lbvh.wgsl:168-232                                         */
+/* ------------------------------------------------------------------------ */
+
+void orc_fill(uint32_t n, uint32_t offset, const uint32_t* ids, const float* mass,
+              const float* pos, const uint32_t* left, const uint32_t* right,
+              const uint32_t* parent, float* com, float* mass_node, float* aabb, float* length) {
+    if (n == 0) return;
+    uint32_t* status = (uint32_t*)calloc(n, sizeof(uint32_t));
+    const uint32_t nm1 = n - 1;
+    /* Exactly n invocations (the reference's padding invocations re-run real
+     * leaves; see lbvh.wgsl:171-176).  Arrival counters are acq_rel. */
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < (int64_t)n; ++g) {
+        uint32_t i = (uint32_t)(((uint64_t)g + offset) % n);
+        uint32_t cur = nm1 + i;
+        uint32_t b = ids[i];
+        float m = mass[b], px = pos[2 * b], py = pos[2 * b + 1];
+        mass_node[cur] = m;
+        com[2 * cur] = px; com[2 * cur + 1] = py;
+        aabb[4 * cur] = px; aabb[4 * cur + 1] = py;
+        aabb[4 * cur + 2] = px; aabb[4 * cur + 3] = py;
+        length[cur] = 0.0f;
+        while (cur != 0u) {
+            uint32_t pidx = parent[cur];
+            if (pidx == cur) break;
+            uint32_t prev = __atomic_fetch_add(&status[pidx], 1u, __ATOMIC_ACQ_REL);
+            if (prev == 0u) break;
+            uint32_t l = left[pidx], r = right[pidx];
+            float lminx = aabb[4 * l], lminy = aabb[4 * l + 1], lmaxx = aabb[4 * l + 2], lmaxy = aabb[4 * l + 3];
+            float rminx = aabb[4 * r], rminy = aabb[4 * r + 1], rmaxx = aabb[4 * r + 2], rmaxy = aabb[4 * r + 3];
+            float minx = fminf(lminx, rminx), miny = fminf(lminy, rminy);
+            float maxx = fmaxf(lmaxx, rmaxx), maxy = fmaxf(lmaxy, rmaxy);
+            aabb[4 * pidx] = minx; aabb[4 * pidx + 1] = miny;
+            aabb[4 * pidx + 2] = maxx; aabb[4 * pidx + 3] = maxy;
+            float ml = mass_node[l], mr = mass_node[r];
+            float tm = ml + mr;
+            mass_node[pidx] = tm;
+            if (tm > 0.0f) {
+                com[2 * pidx] = (com[2 * l] * ml + com[2 * r] * mr) / tm;
+                com[2 * pidx + 1] = (com[2 * l + 1] * ml + com[2 * r + 1] * mr) / tm;
+            } else {
+                com[2 * pidx] = 0.0f;
+                com[2 * pidx + 1] = 0.0f;
+            }
+            float sx = maxx - minx, sy = maxy - miny;
+            length[pidx] = fmaxf(sx, sy);
+            cur = pidx;
+        }
+    }
+    free(status);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Walk: barnes_hut.wgsl:48-111                                              */
+/* ------------------------------------------------------------------------ */
+
+/* Sorted-slot range [first, last] of every node (used for leaf buckets). */
+static void node_ranges(uint32_t n, const uint32_t* left, const uint32_t* right, uint32_t* first,
+                        uint32_t* last) {
+    const uint32_t nm1 = n - 1;
+    for (uint32_t i = 0; i < n; ++i) first[nm1 + i] = last[nm1 + i] = i;
+    if (n < 2) return;
+    /* iterative post-order from the root */
+    uint32_t* st = (uint32_t*)malloc(sizeof(uint32_t) * 2 * (size_t)n);
+    uint8_t* seen = (uint8_t*)calloc(n, 1);
+    int64_t sp = 0;
+    st[sp++] = 0;
+    while (sp > 0) {
+        uint32_t v = st[sp - 1];
+        if (v >= nm1) { sp--; continue; }
+        if (!seen[v]) {
+            seen[v] = 1;
+            st[sp++] = left[v];
+            st[sp++] = right[v];
+        } else {
+            sp--;
+            first[v] = first[left[v]];
+            last[v] = last[right[v]];
+        }
+    }
+    free(st);
+    free(seen);
+}
+
+static inline float soft2(const orc_params* p, float m1, float m2) {
+    if (p->softening == ORC_SOFT_PLUMMER) return p->plummer_eps * p->plummer_eps;
+    float meff = m1 > m2 ? m1 : m2;                                  /* barnes_hut.wgsl:90 */
+    float eps = p->epsilon_multiplier * sqrtf(p->grav_constant * meff * p->delta_time); /* :91 */
+    return eps * eps;
+}
+
+static void walk_impl(const orc_params* p, uint32_t n, const uint32_t* ids, const float* mass,
+                      const float* pos, const float* com, const float* mass_node,
+                      const float* length, const uint32_t* left, const uint32_t* right,
+                      float* acc, uint64_t* visits_out, uint64_t* inter_out) {
+    if (n == 0) return;
+    const uint32_t nm1 = n - 1;
+    const float g = p->grav_constant, theta = p->bh_theta;
+    const int L = p->leaf_size > 1 ? p->leaf_size : 1;
+    uint32_t *first = NULL, *last = NULL;
+    if (L > 1) {
+        first = (uint32_t*)malloc(sizeof(uint32_t) * (2 * (size_t)n - 1));
+        last = (uint32_t*)malloc(sizeof(uint32_t) * (2 * (size_t)n - 1));
+        node_ranges(n, left, right, first, last);
+    }
+    uint64_t tv = 0, ti = 0;
+#pragma omp parallel for num_threads(nthreads(p)) schedule(dynamic, 256) reduction(+ : tv, ti)
+    for (int64_t tid = 0; tid < (int64_t)n; ++tid) {
+        uint32_t body = ids[tid];                        /* barnes_hut.wgsl:56 */
+        float p1x = pos[2 * body], p1y = pos[2 * body + 1], m1 = mass[body];
+        float ax = 0.0f, ay = 0.0f;
+        uint32_t stack[STACK_SIZE];
+        int sp = 0;
+        stack[0] = 0u;
+        while (sp >= 0) {                                /* barnes_hut.wgsl:72 */
+            uint32_t node = stack[sp];
+            sp -= 1;
+            tv++;
+            float p2x = com[2 * node], p2y = com[2 * node + 1], m2 = mass_node[node];
+            float rx = p2x - p1x, ry = p2y - p1y;
+            float d2 = rx * rx + ry * ry;
+            int leaf = node >= nm1;
+            if (leaf && ids[node - nm1] == body) continue; /* barnes_hut.wgsl:83-88 */
+            float inv = 1.0f / sqrtf(d2 + soft2(p, m1, m2));
+            if (leaf || length[node] * inv < theta) {       /* barnes_hut.wgsl:94 */
+                float inv3 = inv * inv * inv;
+                float gm = g * m2;
+                ax += gm * rx * inv3;
+                ay += gm * ry * inv3;
+                ti++;
+            } else if (L > 1 && last[node] - first[node] + 1 <= (uint32_t)L) {
+                /* Extension: direct sum over the bucket's bodies in slot order. */
+                for (uint32_t s = first[node]; s <= last[node]; ++s) {
+                    if (s == (uint32_t)tid) continue;
+                    uint32_t bj = ids[s];
+                    float qx = pos[2 * bj] - p1x, qy = pos[2 * bj + 1] - p1y;
+                    float mj = mass[bj];
+                    float e2 = qx * qx + qy * qy;
+                    float iv = 1.0f / sqrtf(e2 + soft2(p, m1, mj));
+                    float iv3 = iv * iv * iv;
+                    float gmj = g * mj;
+                    ax += gmj * qx * iv3;
+                    ay += gmj * qy * iv3;
+                    ti++;
+                }
+            } else if (sp + 2 < STACK_SIZE) {               /* barnes_hut.wgsl:100-105 */
+                sp += 1;
+                stack[sp] = left[node];
+                sp += 1;
+                stack[sp] = right[node];
+            }
+        }
+        if (acc) {
+            acc[2 * body] = ax;
+            acc[2 * body + 1] = ay;
+        }
+    }
+    if (visits_out) *visits_out = tv;
+    if (inter_out) *inter_out = ti;
+    free(first);
+    free(last);
+}
+
+void orc_walk(const orc_params* p, uint32_t n, const uint32_t* ids, const float* mass,
+              const float* pos, const float* com, const float* mass_node, const float* length,
+              const uint32_t* left, const uint32_t* right, float* acc) {
+    walk_impl(p, n, ids, mass, pos, com, mass_node, length, left, right, acc, NULL, NULL);
+}
+
+void orc_walk_counts(const orc_params* p, uint32_t n, const uint32_t* ids, const float* mass,
+                     const float* pos, const float* com, const float* mass_node,
+                     const float* length, const uint32_t* left, const uint32_t* right,
+                     uint64_t* visits, uint64_t* interactions) {
+    walk_impl(p, n, ids, mass, pos, com, mass_node, length, left, right, NULL, visits,
+              interactions);
+}
+
+/* ------------------------------------------------------------------------ */
+/* FP64 direct sum (accuracy oracle; no reference counterpart)               */
+/* ------------------------------------------------------------------------ */
+
+void orc_direct_sum_fp64(const orc_params* p, uint32_t n, const float* mass, const float* pos,
+                         uint32_t nsample, const uint32_t* sample, double* acc_out) {
+    const double g = p->grav_constant;
+#pragma omp parallel for num_threads(nthreads(p)) schedule(dynamic, 4)
+    for (int64_t k = 0; k < (int64_t)nsample; ++k) {
+        uint32_t i = sample[k];
+        double xi = pos[2 * i], yi = pos[2 * i + 1], mi = mass[i];
+        double ax = 0.0, ay = 0.0;
+        for (uint32_t j = 0; j < n; ++j) {
+            if (j == i) continue;
+            double rx = (double)pos[2 * j] - xi, ry = (double)pos[2 * j + 1] - yi;
+            double mj = mass[j], e2;
+            if (p->softening == ORC_SOFT_PLUMMER) {
+                e2 = (double)p->plummer_eps * (double)p->plummer_eps;
+            } else {
+                double meff = mi > mj ? mi : mj;
+                double eps = (double)p->epsilon_multiplier * sqrt(g * meff * (double)p->delta_time);
+                e2 = eps * eps;
+            }
+            double r2 = rx * rx + ry * ry + e2;
+            double inv = 1.0 / sqrt(r2);
+            double f = g * mj * inv * inv * inv;
+            ax += f * rx;
+            ay += f * ry;
+        }
+        acc_out[2 * k] = ax;
+        acc_out[2 * k + 1] = ay;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Whole-step state (simulation.ts:82-91 buffers, :386-425 stage order)      */
+/* ------------------------------------------------------------------------ */
+
+struct orc_state {
+    orc_params p;
+    uint32_t n;
+    float *mass, *pos, *vel, *acc;
+    int acc_valid;
+    uint64_t* codes;
+    uint32_t *ids, *left, *right, *parent;
+    float *com, *mass_node, *aabb, *length;
+};
+
+orc_state* orc_create(const orc_params* p, uint32_t n, const float* mass, const float* pos,
+                      const float* vel) {
+    orc_state* s = (orc_state*)calloc(1, sizeof(orc_state));
+    s->p = *p;
+    s->n = n;
+    size_t nn = n ? 2 * (size_t)n - 1 : 1;
+    size_t nb = n ? n : 1;
+    s->mass = (float*)malloc(sizeof(float) * nb);
+    s->pos = (float*)malloc(sizeof(float) * 2 * nb);
+    s->vel = (float*)malloc(sizeof(float) * 2 * nb);
+    s->acc = (float*)calloc(2 * nb, sizeof(float));
+    s->codes = (uint64_t*)malloc(sizeof(uint64_t) * nb);
+    s->ids = (uint32_t*)malloc(sizeof(uint32_t) * nb);
+    s->left = (uint32_t*)calloc(nn, sizeof(uint32_t));
+    s->right = (uint32_t*)calloc(nn, sizeof(uint32_t));
+    s->parent = (uint32_t*)calloc(nn, sizeof(uint32_t));
+    s->com = (float*)calloc(2 * nn, sizeof(float));
+    s->mass_node = (float*)calloc(nn, sizeof(float));
+    s->aabb = (float*)calloc(4 * nn, sizeof(float));
+    s->length = (float*)calloc(nn, sizeof(float));
+    if (n) {
+        memcpy(s->mass, mass, sizeof(float) * n);
+        memcpy(s->pos, pos, sizeof(float) * 2 * n);
+        memcpy(s->vel, vel, sizeof(float) * 2 * n);
+    }
+    return s;
+}
+
+void orc_destroy(orc_state* s) {
+    if (!s) return;
+    free(s->mass); free(s->pos); free(s->vel); free(s->acc);
+    free(s->codes); free(s->ids); free(s->left); free(s->right); free(s->parent);
+    free(s->com); free(s->mass_node); free(s->aabb); free(s->length);
+    free(s);
+}
+
+/* Morton -> sort -> build -> fill (simulation.ts:395-410). */
+static void build_tree(orc_state* s) {
+    orc_domain dom;
+    orc_domain_compute(&s->p, s->n, s->pos, &dom);
+    orc_morton(&s->p, &dom, s->n, s->pos, s->codes, s->ids);
+    radix_sort_impl(s->n, s->codes, s->ids, s->p.morton_bits, nthreads(&s->p));
+    orc_build(s->n, s->p.morton_bits, s->codes, s->left, s->right, s->parent);
+    orc_fill(s->n, 0, s->ids, s->mass, s->pos, s->left, s->right, s->parent, s->com,
+             s->mass_node, s->aabb, s->length);
+}
+
+static void forces(orc_state* s) {
+    build_tree(s);
+    walk_impl(&s->p, s->n, s->ids, s->mass, s->pos, s->com, s->mass_node, s->length, s->left,
+              s->right, s->acc, NULL, NULL);
+    s->acc_valid = 1;
+}
+
+void orc_accelerations(orc_state* s, float* acc) {
+    forces(s);
+    if (acc) memcpy(acc, s->acc, sizeof(float) * 2 * s->n);
+}
+
+void orc_step(orc_state* s, uint32_t nsteps) {
+    const uint32_t n = s->n;
+    const float dt = s->p.delta_time;
+    const int nt = nthreads(&s->p);
+    if (n == 0) return;
+    for (uint32_t step = 0; step < nsteps; ++step) {
+        if (s->p.integrator == ORC_INT_LEAPFROG_KDK) {
+            /* Extension: kick-drift-kick with the force of the previous step cached. */
+            const float hdt = 0.5f * dt;
+            if (!s->acc_valid) forces(s);
+#pragma omp parallel for num_threads(nt) schedule(static)
+            for (int64_t b = 0; b < (int64_t)n; ++b) {
+                float vx = s->vel[2 * b] + s->acc[2 * b] * hdt;
+                float vy = s->vel[2 * b + 1] + s->acc[2 * b + 1] * hdt;
+                s->vel[2 * b] = vx;
+                s->vel[2 * b + 1] = vy;
+                s->pos[2 * b] = s->pos[2 * b] + vx * dt;
+                s->pos[2 * b + 1] = s->pos[2 * b + 1] + vy * dt;
+            }
+            forces(s);
+#pragma omp parallel for num_threads(nt) schedule(static)
+            for (int64_t b = 0; b < (int64_t)n; ++b) {
+                s->vel[2 * b] = s->vel[2 * b] + s->acc[2 * b] * hdt;
+                s->vel[2 * b + 1] = s->vel[2 * b + 1] + s->acc[2 * b + 1] * hdt;
+            }
+        } else {
+            /* Reference: kick (barnes_hut.wgsl:110) then drift (:119-120). */
+            forces(s);
+#pragma omp parallel for num_threads(nt) schedule(static)
+            for (int64_t b = 0; b < (int64_t)n; ++b) {
+                float vx = s->vel[2 * b] + s->acc[2 * b] * dt;
+                float vy = s->vel[2 * b + 1] + s->acc[2 * b + 1] * dt;
+                s->vel[2 * b] = vx;
+                s->vel[2 * b + 1] = vy;
+                s->pos[2 * b] = s->pos[2 * b] + vx * dt;
+                s->pos[2 * b + 1] = s->pos[2 * b + 1] + vy * dt;
+            }
+            s->acc_valid = 0;
+        }
+    }
+}
+
+void orc_get_state(const orc_state* s, float* pos, float* vel) {
+    if (pos) memcpy(pos, s->pos, sizeof(float) * 2 * s->n);
+    if (vel) memcpy(vel, s->vel, sizeof(float) * 2 * s->n);
+}
+
+void orc_get_tree(const orc_state* s, uint64_t* codes, uint32_t* ids, uint32_t* left,
+                  uint32_t* right, uint32_t* parent, float* com, float* mass_node, float* aabb,
+                  float* length) {
+    size_t n = s->n, nn = n ? 2 * n - 1 : 0;
+    if (codes) memcpy(codes, s->codes, sizeof(uint64_t) * n);
+    if (ids) memcpy(ids, s->ids, sizeof(uint32_t) * n);
+    if (left) memcpy(left, s->left, sizeof(uint32_t) * nn);
+    if (right) memcpy(right, s->right, sizeof(uint32_t) * nn);
+    if (parent) memcpy(parent, s->parent, sizeof(uint32_t) * nn);
+    if (com) memcpy(com, s->com, sizeof(float) * 2 * nn);
+    if (mass_node) memcpy(mass_node, s->mass_node, sizeof(float) * nn);
+    if (aabb) memcpy(aabb, s->aabb, sizeof(float) * 4 * nn);
+    if (length) memcpy(length, s->length, sizeof(float) * nn);
+}
+
+uint32_t orc_num_bodies(const orc_state* s) { return s->n; }

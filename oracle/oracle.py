@@ -1,0 +1,235 @@
+"""ctypes wrapper of the oracle library (libbh_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, the smoke check and the CPU
+baseline of bench.py as the checker.  The engine never imports this module.
+The C restatement it wraps follows lbvh.wgsl / barnes_hut.wgsl of the
+reference line by line (see bh_oracle.h for the citations).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbh_oracle.so")
+
+SOFT = {"reference": 0, "plummer": 1}
+DOMAIN = {"fixed2000": 0, "bbox": 1}
+INTEGRATOR = {"symplectic-euler": 0, "leapfrog-kdk": 1}
+
+
+class OrcParams(ctypes.Structure):
+    _fields_ = [
+        ("grav_constant", ctypes.c_float),
+        ("delta_time", ctypes.c_float),
+        ("epsilon_multiplier", ctypes.c_float),
+        ("bh_theta", ctypes.c_float),
+        ("softening", ctypes.c_int),
+        ("plummer_eps", ctypes.c_float),
+        ("morton_bits", ctypes.c_int),
+        ("morton_domain", ctypes.c_int),
+        ("integrator", ctypes.c_int),
+        ("leaf_size", ctypes.c_int),
+        ("threads", ctypes.c_int),
+    ]
+
+
+class OrcDomain(ctypes.Structure):
+    _fields_ = [("lo_x", ctypes.c_float), ("lo_y", ctypes.c_float),
+                ("extent", ctypes.c_float), ("pow2_exp", ctypes.c_int)]
+
+
+_lib = None
+_P = ctypes.c_void_p
+
+
+def load() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("oracle_build", os.path.join(HERE, "build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build_oracle()
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER(OrcParams)
+    sig = {
+        "orc_domain_compute": (None, [P, ctypes.c_uint32, _P, ctypes.POINTER(OrcDomain)]),
+        "orc_morton": (None, [P, ctypes.POINTER(OrcDomain), ctypes.c_uint32, _P, _P, _P]),
+        "orc_sort": (None, [ctypes.c_uint32, _P, _P]),
+        "orc_build": (None, [ctypes.c_uint32, ctypes.c_int, _P, _P, _P, _P]),
+        "orc_fill": (None, [ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P,
+                            _P, _P]),
+        "orc_walk": (None, [P, ctypes.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+        "orc_walk_counts": (None, [P, ctypes.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+        "orc_direct_sum_fp64": (None, [P, ctypes.c_uint32, _P, _P, ctypes.c_uint32, _P, _P]),
+        "orc_create": (_P, [P, ctypes.c_uint32, _P, _P, _P]),
+        "orc_destroy": (None, [_P]),
+        "orc_step": (None, [_P, ctypes.c_uint32]),
+        "orc_accelerations": (None, [_P, _P]),
+        "orc_get_state": (None, [_P, _P, _P]),
+        "orc_get_tree": (None, [_P] + [_P] * 9),
+        "orc_num_bodies": (ctypes.c_uint32, [_P]),
+        "orc_max_threads": (ctypes.c_int, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def params(G=1.0, dt=0.1 / 60.0, eps_mult=1.0, theta=0.6, softening="reference",
+           plummer_eps=1e-3, morton_bits=32, morton_domain="fixed2000",
+           integrator="symplectic-euler", leaf_size=1, threads=0) -> OrcParams:
+    return OrcParams(G, dt, eps_mult, theta, SOFT[softening], plummer_eps, morton_bits,
+                     DOMAIN[morton_domain], INTEGRATOR[integrator], leaf_size, threads)
+
+
+def params_from_config(cfg, threads: int = 0) -> OrcParams:
+    """OrcParams equal to an engine Config (duck-typed: the field names of config.ts)."""
+    return params(G=cfg.gravConstant, dt=cfg.deltaTime, eps_mult=cfg.epsilonMultiplier,
+                  theta=cfg.bhTheta, softening=cfg.softening, plummer_eps=cfg.plummerEps,
+                  morton_bits=cfg.mortonBits, morton_domain=cfg.mortonDomain,
+                  integrator=cfg.integrator, leaf_size=cfg.leafSize, threads=threads)
+
+
+def f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a.reshape(shape) if shape is not None else a
+
+
+def morton(p: OrcParams, pos) -> tuple[np.ndarray, np.ndarray]:
+    lib = load()
+    pos = f32(pos, (-1, 2))
+    n = pos.shape[0]
+    dom = OrcDomain()
+    lib.orc_domain_compute(ctypes.byref(p), n, _p(pos), ctypes.byref(dom))
+    codes = np.empty(n, np.uint64)
+    ids = np.empty(n, np.uint32)
+    lib.orc_morton(ctypes.byref(p), ctypes.byref(dom), n, _p(pos), _p(codes), _p(ids))
+    return codes, ids
+
+
+def sort(codes, ids):
+    lib = load()
+    codes = np.ascontiguousarray(codes, np.uint64).copy()
+    ids = np.ascontiguousarray(ids, np.uint32).copy()
+    lib.orc_sort(codes.size, _p(codes), _p(ids))
+    return codes, ids
+
+
+def build(codes, bits: int = 32):
+    lib = load()
+    codes = np.ascontiguousarray(codes, np.uint64)
+    n = codes.size
+    nn = max(2 * n - 1, 1)
+    left = np.zeros(nn, np.uint32)
+    right = np.zeros(nn, np.uint32)
+    parent = np.zeros(nn, np.uint32)
+    lib.orc_build(n, bits, _p(codes), _p(left), _p(right), _p(parent))
+    return left, right, parent
+
+
+def fill(ids, mass, pos, left, right, parent, offset: int = 0):
+    lib = load()
+    n = len(ids)
+    nn = max(2 * n - 1, 1)
+    com = np.zeros((nn, 2), np.float32)
+    mnode = np.zeros(nn, np.float32)
+    aabb = np.zeros((nn, 4), np.float32)
+    length = np.zeros(nn, np.float32)
+    lib.orc_fill(n, offset, _p(np.ascontiguousarray(ids, np.uint32)), _p(f32(mass)),
+                 _p(f32(pos, (-1, 2))), _p(left), _p(right), _p(parent), _p(com), _p(mnode),
+                 _p(aabb), _p(length))
+    return com, mnode, aabb, length
+
+
+def walk(p: OrcParams, ids, mass, pos, com, mnode, length, left, right):
+    lib = load()
+    n = len(ids)
+    acc = np.zeros((n, 2), np.float32)
+    lib.orc_walk(ctypes.byref(p), n, _p(np.ascontiguousarray(ids, np.uint32)), _p(f32(mass)),
+                 _p(f32(pos, (-1, 2))), _p(com), _p(mnode), _p(length), _p(left), _p(right),
+                 _p(acc))
+    return acc
+
+
+def walk_counts(p: OrcParams, ids, mass, pos, com, mnode, length, left, right):
+    lib = load()
+    n = len(ids)
+    v = ctypes.c_uint64()
+    i = ctypes.c_uint64()
+    lib.orc_walk_counts(ctypes.byref(p), n, _p(np.ascontiguousarray(ids, np.uint32)),
+                        _p(f32(mass)), _p(f32(pos, (-1, 2))), _p(com), _p(mnode), _p(length),
+                        _p(left), _p(right), ctypes.byref(v), ctypes.byref(i))
+    return int(v.value), int(i.value)
+
+
+def direct_sum_fp64(p: OrcParams, mass, pos, sample) -> np.ndarray:
+    lib = load()
+    mass = f32(mass)
+    pos = f32(pos, (-1, 2))
+    sample = np.ascontiguousarray(sample, np.uint32)
+    out = np.zeros((sample.size, 2), np.float64)
+    lib.orc_direct_sum_fp64(ctypes.byref(p), mass.size, _p(mass), _p(pos), sample.size,
+                            _p(sample), _p(out))
+    return out
+
+
+class State:
+    """Whole-step oracle run (simulation.ts:386-425 stage order)."""
+
+    def __init__(self, p: OrcParams, mass, pos, vel):
+        self.lib = load()
+        self.p = p
+        self.mass = f32(mass)
+        self.n = self.mass.size
+        self._h = self.lib.orc_create(ctypes.byref(p), self.n, _p(self.mass),
+                                      _p(f32(pos, (-1, 2))), _p(f32(vel, (-1, 2))))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self.lib.orc_destroy(h)
+            self._h = None
+
+    def step(self, nsteps: int = 1) -> None:
+        self.lib.orc_step(self._h, nsteps)
+
+    def accelerations(self) -> np.ndarray:
+        acc = np.zeros((self.n, 2), np.float32)
+        self.lib.orc_accelerations(self._h, _p(acc))
+        return acc
+
+    def state(self):
+        pos = np.zeros((self.n, 2), np.float32)
+        vel = np.zeros((self.n, 2), np.float32)
+        self.lib.orc_get_state(self._h, _p(pos), _p(vel))
+        return pos, vel
+
+    def tree(self) -> dict:
+        n = self.n
+        nn = max(2 * n - 1, 1)
+        codes = np.zeros(n, np.uint64)
+        ids = np.zeros(n, np.uint32)
+        left = np.zeros(nn, np.uint32)
+        right = np.zeros(nn, np.uint32)
+        parent = np.zeros(nn, np.uint32)
+        com = np.zeros((nn, 2), np.float32)
+        mnode = np.zeros(nn, np.float32)
+        aabb = np.zeros((nn, 4), np.float32)
+        length = np.zeros(nn, np.float32)
+        self.lib.orc_get_tree(self._h, _p(codes), _p(ids), _p(left), _p(right), _p(parent),
+                              _p(com), _p(mnode), _p(aabb), _p(length))
+        return dict(codes=codes, ids=ids, left=left, right=right, parent=parent, com=com,
+                    mass=mnode, aabb=aabb, length=length)

@@ -1,0 +1,175 @@
+"""GPU parity: the CUDA engine against the oracle on the same seeded inputs.
+
+Bit-exact: Morton codes, the sorted permutation, left/right/parent arrays,
+node AABBs and lengths.  Tolerances (FP32):
+  node mass   |dm| <= 1e-5 |m|                    (FP64 top levels vs f32 reference)
+  node COM    |dc| <= 1e-5 (|c| + length)
+  acceleration (reference walk): median relative error <= 1e-5 and at most
+    1% of bodies above 1e-3 (those are theta-boundary criterion flips caused
+    by rsqrt vs 1/sqrt rounding; the count is reported).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SENT = 0xFFFFFFFF
+
+
+def make_sim(bh, n, scenario="default", seed=1, **cfg):
+    sim = bh.Simulation(bh.Config(**cfg))
+    sim.setNumBodies(n)
+    sim.setScenario(scenario, seed)
+    return sim
+
+
+def oracle_params(orc, sim):
+    return orc.params_from_config(sim.config)
+
+
+def compare_tree(orc, sim, check_values=True):
+    n = sim.getNumBodies()
+    mass, pos, vel = sim.download()
+    acc = sim.computeAccelerations()
+    t = sim.tree()
+    st = orc.State(oracle_params(orc, sim), mass, pos, vel)
+    acc_ref = st.accelerations()
+    r = st.tree()
+    assert (t["codes"].astype(np.uint64) == r["codes"]).all(), "Morton codes differ"
+    assert (t["ids"] == r["ids"]).all(), "sorted permutation differs"
+    assert (t["parent"] == r["parent"]).all(), "parent array differs"
+    if n > 1:
+        assert (t["children"][:, 0] == r["left"][: n - 1]).all(), "left children differ"
+        assert (t["children"][:, 1] == r["right"][: n - 1]).all(), "right children differ"
+        assert (t["aabb"] == r["aabb"][: n - 1]).all(), "AABBs differ"
+        assert (t["node4"][: n - 1, 3] == r["length"][: n - 1]).all(), "lengths differ"
+    if check_values:
+        m_gpu, m_ref = t["node4"][:, 2], r["mass"]
+        assert np.all(np.abs(m_gpu - m_ref) <= 1e-5 * np.abs(m_ref) + 1e-30)
+        c_gpu, c_ref = t["node4"][:, :2], r["com"]
+        scale = np.abs(c_ref).max(1) + r["length"]
+        assert np.all(np.abs(c_gpu - c_ref).max(1) <= 1e-5 * scale + 1e-30)
+    return acc, acc_ref
+
+
+def acc_errors(acc, acc_ref):
+    num = np.linalg.norm(acc.astype(np.float64) - acc_ref, axis=1)
+    den = np.linalg.norm(acc_ref.astype(np.float64), axis=1)
+    den = np.maximum(den, 1e-6 * np.median(den) + 1e-30)
+    return num / den
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 63, 64, 65, 1000, 4097, 20000])
+def test_reference_mode_tree_and_forces(bh, orc, n):
+    sim = make_sim(bh, n, "default", seed=n)
+    acc, acc_ref = compare_tree(orc, sim)
+    if n > 1:
+        err = acc_errors(acc, acc_ref)
+        assert np.median(err) <= 1e-5
+        assert (err > 1e-3).mean() <= 0.01
+    sim.close()
+
+
+@pytest.mark.parametrize("scenario", ["two-clusters", "planetary-disk"])
+def test_reference_scenarios(bh, orc, scenario):
+    sim = make_sim(bh, 30000, scenario, seed=5)
+    acc, acc_ref = compare_tree(orc, sim)
+    err = acc_errors(acc, acc_ref)
+    assert np.median(err) <= 1e-5
+    assert (err > 1e-3).mean() <= 0.01
+    sim.close()
+
+
+@pytest.mark.parametrize("cfg", [
+    dict(mortonDomain="bbox"),
+    dict(mortonBits=64),
+    dict(softening="plummer", plummerEps=1e-3, mortonDomain="bbox", bhTheta=0.5),
+    dict(softening="plummer", plummerEps=1e-3, mortonBits=64, leafSize=8, bhTheta=0.5),
+])
+def test_extension_modes_tree_and_forces(bh, orc, cfg):
+    sim = make_sim(bh, 20000, "colliding-disks", seed=3, **cfg)
+    acc, acc_ref = compare_tree(orc, sim)
+    err = acc_errors(acc, acc_ref)
+    assert np.median(err) <= 1e-5
+    assert (err > 1e-3).mean() <= 0.01
+    sim.close()
+
+
+def test_duplicates_gaussian_mixture_64bit(bh, orc):
+    sim = make_sim(bh, 50000, "gaussian-mixture", seed=9, mortonBits=64, softening="plummer",
+                   plummerEps=1e-4, bhTheta=0.5)
+    acc, acc_ref = compare_tree(orc, sim)
+    err = acc_errors(acc, acc_ref)
+    assert np.median(err) <= 1e-5
+    assert (err > 1e-3).mean() <= 0.01
+    sim.close()
+
+
+@pytest.mark.parametrize("integrator", ["symplectic-euler", "leapfrog-kdk"])
+def test_steps_match_oracle(bh, orc, integrator):
+    sim = make_sim(bh, 5000, "default", seed=2, integrator=integrator, mortonDomain="bbox")
+    mass, pos, vel = sim.download()
+    st = orc.State(oracle_params(orc, sim), mass, pos, vel)
+    sim.step(3)
+    sim.sync()
+    st.step(3)
+    _, p_gpu, v_gpu = sim.download()
+    p_ref, v_ref = st.state()
+    vscale = np.abs(v_ref).max()
+    assert np.abs(v_gpu - v_ref).max() <= 1e-4 * vscale
+    assert np.abs(p_gpu - p_ref).max() <= 1e-5 * (np.abs(p_ref).max() + 1)
+    sim.close()
+
+
+def test_large_tree_properties_800k(bh):
+    # Full-size case: size-independent properties instead of an oracle run.
+    sim = make_sim(bh, 800_000, "colliding-disks", seed=11, mortonDomain="bbox",
+                   softening="plummer", bhTheta=0.5)
+    mass, pos, vel = sim.download()
+    sim.computeAccelerations()
+    t = sim.tree()
+    n = 800_000
+    codes, ids = t["codes"], t["ids"]
+    assert (np.diff(codes.astype(np.int64)) >= 0).all()
+    assert np.array_equal(np.sort(ids), np.arange(n, dtype=np.uint32))
+    # stable: equal codes keep ascending ids
+    same = codes[1:] == codes[:-1]
+    assert (ids[1:][same] > ids[:-1][same]).all()
+    ch, par = t["children"], t["parent"]
+    assert par[0] == SENT
+    assert (par[ch[:, 0]] == np.arange(n - 1)).all() and (par[ch[:, 1]] == np.arange(n - 1)).all()
+    cnt = np.bincount(ch.reshape(-1), minlength=2 * n - 1)
+    assert cnt[0] == 0 and (cnt[1:] == 1).all()
+    # mass conservation at the root (FP64 top levels)
+    np.testing.assert_allclose(t["node4"][0, 2], mass.astype(np.float64).sum(), rtol=1e-6)
+    sim.close()
+
+
+def test_graph_and_direct_paths_agree(bh):
+    outs = []
+    for graphs in (True, False):
+        sim = make_sim(bh, 10000, "two-clusters", seed=4, useGraphs=graphs)
+        sim.step(4)
+        sim.sync()
+        outs.append(sim.download())
+        sim.close()
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+
+
+def test_profile_and_kernel_count(bh):
+    sim = make_sim(bh, 50000, "default", seed=1)
+    sim.profile_begin(5)
+    sim.step(5)
+    ms, steps = sim.profile_end()
+    assert steps == 5
+    assert all(v >= 0 for v in ms.values()) and ms["walk"] > 0
+    assert sim.kernels_per_step() == 1 + 4 + 1 + 1  # encode, 4 sort passes, build+fill, walk
+    sim.close()
+
+
+def test_unknown_scenario_raises(bh):
+    sim = bh.Simulation()
+    with pytest.raises(bh.BhError, match="Unknown scenario: nope"):
+        sim.setScenario("nope")
+    sim.close()

@@ -1,0 +1,11 @@
+"""B200-native Barnes-Hut engine for the per-step compute pipeline of the
+ElliottF05/webgpu-fluid-sim N-body simulator.
+
+The package directory name has hyphens, so load it with
+``importlib.import_module("webgpu-fluid-sim_b200")`` after putting the
+repository root on ``sys.path``.
+"""
+from ._lib import BhError, load  # noqa: F401
+from .config import WORKLOADS, Config, getDefaultConfig  # noqa: F401
+from .simulation import (SCENARIOS, CommandBuffer, SimBuffers, Simulation,  # noqa: F401
+                         generate_scenario, submit)

@@ -1,0 +1,108 @@
+// bh_internal.cuh -- device data layout and kernel launchers of the engine.
+//
+// Stage map (reference: src/simulation.ts:394-420, one step):
+//   morton.cu  bounding box (extension) + Morton encode + digit histograms
+//   sort.cu    onesweep LSD radix sort of (key, id) pairs
+//   tree.cu    fused bottom-up hierarchy build + mass/COM/AABB fill
+//   walk.cu    warp-cooperative theta-criterion walk + kick (+ drift)
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bh {
+
+constexpr uint32_t kSentinel = 0xFFFFFFFFu;
+constexpr int kStackSize = 256;  // barnes_hut.wgsl:67
+// Nodes with at least this many bodies aggregate mass/COM in FP64.
+constexpr uint32_t kFp64MinBodies = 1024;
+
+// Sort tiling.
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 256;
+
+// Device error word bits (read by the host after a sync).
+constexpr uint32_t kErrLookbackSpin = 1u << 0;  // decoupled look-back gave up waiting
+constexpr uint32_t kErrStackOverflow = 1u << 1; // walk stack would have overflowed (children dropped)
+constexpr uint32_t kErrTreeSpin = 1u << 2;
+
+// Walk modes.
+enum WalkMode : int {
+    kWalkForces = 0,       // acc[b] = a
+    kWalkEulerKickDrift,   // v += a*dt; x += v*dt (reference, barnes_hut.wgsl:110,119-120)
+    kWalkKdkClose,         // v += a*dt/2; acc[b] = a (leapfrog closing kick)
+};
+
+struct WalkParams {
+    uint32_t n;
+    float g;
+    float theta;
+    float dt;
+    float eps_coef;   // reference softening: eps^2 = eps_coef * max(m1, m2)
+    float eps2;       // Plummer softening: eps^2 (constant)
+    int plummer;      // 1 = Plummer
+    int leaf_size;    // bucket size (1 = reference walk)
+    int mode;         // WalkMode
+    int count;        // 1 = instrumented launch: accumulate visit/interaction counters
+    unsigned long long* counters;  // {node visits, interactions} when count == 1
+};
+
+// Per-step scratch that must start at zero.  One memset clears it.
+struct StepScratch {
+    uint32_t hist[8][kRadix];  // digit histograms per pass
+    uint32_t tile_ctr[8];      // dynamic tile counters per pass
+    uint32_t bbox[4];          // ordered-int max of {-minx, -miny, maxx, maxy} (see morton.cu)
+    unsigned long long walk_counts[2];  // instrumented walk: {node visits, interactions}
+};
+
+struct DeviceBuffers {
+    uint32_t n = 0;
+    uint32_t capacity = 0;  // bodies allocated
+    int key_bytes = 4;      // 4 or 8
+    // bodies, original order (simulation.ts:82-87)
+    float* mass = nullptr;
+    float2* pos = nullptr;
+    float2* vel = nullptr;
+    float2* acc = nullptr;
+    float* radius = nullptr;
+    // sort
+    void* codes = nullptr;      // sorted keys after a step
+    void* codes_alt = nullptr;
+    uint32_t* ids = nullptr;    // sorted permutation after a step
+    uint32_t* ids_alt = nullptr;
+    // tree
+    float4* node4 = nullptr;     // 2n-1 {com.x, com.y, mass, length}
+    uint2* children = nullptr;   // n-1 {left, right}
+    uint32_t* parent = nullptr;  // 2n-1
+    float4* aabb = nullptr;      // n-1 {min.x, min.y, max.x, max.y}
+    uint2* range = nullptr;      // n-1 {first slot, last slot}
+    double2* big = nullptr;      // 2(n-1) FP64 {mass, mass*x}, {mass*y, 0} for big nodes
+    uint32_t* bound = nullptr;   // n-1 exchange slots, kSentinel between steps
+    // scratch
+    StepScratch* scratch = nullptr;
+    uint32_t* status = nullptr;  // look-back status: passes * tiles * 256
+    uint32_t tiles = 0;
+    uint32_t* err = nullptr;     // device error word
+};
+
+// ---- launchers (all asynchronous on `s`) --------------------------------
+// morton.cu
+void launch_bbox(const DeviceBuffers& b, cudaStream_t s);
+// domain: 0 fixed2000, 1 bbox; key_bytes 4 or 8.
+void launch_encode(const DeviceBuffers& b, int domain, cudaStream_t s);
+// leapfrog opening kick + drift: v += a*hdt; x += v*dt (original order)
+void launch_kick_drift(const DeviceBuffers& b, float dt, cudaStream_t s);
+// sort.cu
+void launch_sort(const DeviceBuffers& b, cudaStream_t s);
+cudaError_t sort_init_attributes();
+int sort_passes(const DeviceBuffers& b);
+// tree.cu
+void launch_build_fill(const DeviceBuffers& b, int fp64_levels, cudaStream_t s);
+void init_bound(const DeviceBuffers& b, cudaStream_t s);
+// walk.cu
+void launch_walk(const DeviceBuffers& b, const WalkParams& p, int block, cudaStream_t s);
+
+}  // namespace bh

@@ -1,0 +1,653 @@
+// engine.cu -- the C ABI of include/bh.h: handle lifetime, device buffers,
+// stream-ordered steps replayed from CUDA graphs, profiling and errors.
+//
+// Reference host class: Simulation (src/simulation.ts:39-433).  Buffers
+// (:68-104), scenario set-up (:227-374), metadata (:212-225) and the per-frame
+// command encoding (:386-425) map onto bh_create / bh_set_* / bh_step here.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bh.h"
+#include "bh_internal.cuh"
+
+namespace bh {
+int generate_scenario(const char* name, uint32_t n, uint64_t seed, float grav_constant,
+                      float* mass, float* pos, float* vel, float* radius_mul);
+}
+
+using bh::DeviceBuffers;
+
+static constexpr int kMarkers = 6;  // stage boundaries of one step
+static constexpr uint32_t kMaxBodies = (1u << 30) - 1;
+
+struct bh_sim {
+    bh_config cfg{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t n = 50000;  // simulation.ts:60
+    std::string scenario = "default";
+    uint64_t seed = 0;
+    DeviceBuffers b;
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    bool acc_valid = false;
+    // graphs: [0] plain, [1] with event-record nodes at the stage boundaries
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    cudaGraphNode_t ev_node[kMarkers] = {};
+    cudaEvent_t markers[kMarkers] = {};
+    // profiling
+    bool profiling = false;
+    uint32_t prof_max = 0, prof_used = 0;
+    std::vector<cudaEvent_t> prof_ev;
+    std::string err;
+};
+
+static thread_local std::string g_err;
+
+static int fail(bh_sim* s, int code, const std::string& msg) {
+    if (s) s->err = msg;
+    g_err = msg;
+    return code;
+}
+
+static int cuda_fail(bh_sim* s, cudaError_t e, const char* what) {
+    int code = (e == cudaErrorMemoryAllocation) ? BH_ERR_OUT_OF_MEMORY : BH_ERR_CUDA;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) code = BH_ERR_NO_DEVICE;
+    return fail(s, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define BH_CUDA(s, expr)                                 \
+    do {                                                 \
+        cudaError_t _e = (expr);                         \
+        if (_e != cudaSuccess) return cuda_fail(s, _e, #expr); \
+    } while (0)
+
+// ---- configuration --------------------------------------------------------
+
+extern "C" int bh_default_config(bh_config* out) {
+    if (!out) return fail(nullptr, BH_ERR_INVALID_ARGUMENT, "bh_default_config: null output");
+    std::memset(out, 0, sizeof(*out));
+    // config.ts:10-14
+    out->grav_constant = 1.0f;
+    out->bh_theta = 0.6f;
+    out->substeps = 1;
+    out->delta_time = (float)(0.1 * 1.0 / (60.0 * 1.0));
+    out->epsilon_multiplier = 1.0f;
+    out->softening = BH_SOFTENING_REFERENCE;
+    out->plummer_eps = 1e-3f;
+    out->morton_bits = 32;
+    out->morton_domain = BH_DOMAIN_FIXED2000;
+    out->integrator = BH_INTEGRATOR_SYMPLECTIC_EULER;
+    out->leaf_size = 1;
+    out->walk_block = 0;
+    out->device = 0;
+    out->use_graphs = 1;
+    out->fp64_levels = 1;
+    return BH_OK;
+}
+
+static int validate_config(bh_sim* s, const bh_config& c) {
+    if (c.morton_bits != 32 && c.morton_bits != 64)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "morton_bits must be 32 or 64");
+    if (c.morton_domain != BH_DOMAIN_FIXED2000 && c.morton_domain != BH_DOMAIN_BBOX)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "unknown morton_domain");
+    if (c.softening != BH_SOFTENING_REFERENCE && c.softening != BH_SOFTENING_PLUMMER)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "unknown softening");
+    if (c.integrator != BH_INTEGRATOR_SYMPLECTIC_EULER && c.integrator != BH_INTEGRATOR_LEAPFROG_KDK)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "unknown integrator");
+    if (c.substeps < 1) return fail(s, BH_ERR_INVALID_ARGUMENT, "substeps must be >= 1");
+    if (c.leaf_size < 1 || c.leaf_size > 64)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "leaf_size must be in [1, 64]");
+    if (!(c.delta_time == c.delta_time) || !(c.bh_theta >= 0.0f))
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "delta_time must be a number and bh_theta >= 0");
+    return BH_OK;
+}
+
+// ---- buffers --------------------------------------------------------------
+
+static void destroy_graphs(bh_sim* s) {
+    for (int v = 0; v < 2; ++v) {
+        if (s->exec[v]) cudaGraphExecDestroy(s->exec[v]);
+        if (s->graph[v]) cudaGraphDestroy(s->graph[v]);
+        s->exec[v] = nullptr;
+        s->graph[v] = nullptr;
+    }
+}
+
+static void free_buffers(bh_sim* s) {
+    destroy_graphs(s);
+    if (s->arena) cudaFree(s->arena);
+    s->arena = nullptr;
+    s->arena_bytes = 0;
+    s->b = DeviceBuffers();
+}
+
+struct Carver {
+    size_t off = 0;
+    template <typename T>
+    size_t take(size_t count) {
+        size_t o = off;
+        off += (count * sizeof(T) + 255) & ~(size_t)255;
+        return o;
+    }
+};
+
+static int alloc_buffers(bh_sim* s, uint32_t n) {
+    free_buffers(s);
+    const int kb = s->cfg.morton_bits / 8;
+    const size_t nn = n ? 2 * (size_t)n - 1 : 1, ni = n > 1 ? (size_t)n - 1 : 1, nb = n ? n : 1;
+    const uint32_t tiles = (uint32_t)((n + bh::kSortTile - 1) / bh::kSortTile);
+    Carver c;
+    size_t o_mass = c.take<float>(nb), o_pos = c.take<float2>(nb), o_vel = c.take<float2>(nb);
+    size_t o_acc = c.take<float2>(nb), o_rad = c.take<float>(nb);
+    size_t o_codes = c.take<uint8_t>(nb * kb), o_codes2 = c.take<uint8_t>(nb * kb);
+    size_t o_ids = c.take<uint32_t>(nb), o_ids2 = c.take<uint32_t>(nb);
+    size_t o_node4 = c.take<float4>(nn), o_child = c.take<uint2>(ni), o_parent = c.take<uint32_t>(nn);
+    size_t o_aabb = c.take<float4>(ni), o_range = c.take<uint2>(ni), o_big = c.take<double2>(2 * ni);
+    size_t o_bound = c.take<uint32_t>(ni);
+    size_t o_scr = c.take<bh::StepScratch>(1);
+    size_t o_status = c.take<uint32_t>((size_t)kb * (tiles ? tiles : 1) * bh::kRadix);
+    size_t o_err = c.take<uint32_t>(1);
+    void* arena = nullptr;
+    cudaError_t e = cudaMalloc(&arena, c.off);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(s, e, "cudaMalloc(body and tree buffers)");
+    }
+    s->arena = arena;
+    s->arena_bytes = c.off;
+    char* a = (char*)arena;
+    DeviceBuffers& b = s->b;
+    b.n = n;
+    b.capacity = n;
+    b.key_bytes = kb;
+    b.mass = (float*)(a + o_mass);
+    b.pos = (float2*)(a + o_pos);
+    b.vel = (float2*)(a + o_vel);
+    b.acc = (float2*)(a + o_acc);
+    b.radius = (float*)(a + o_rad);
+    b.codes = a + o_codes;
+    b.codes_alt = a + o_codes2;
+    b.ids = (uint32_t*)(a + o_ids);
+    b.ids_alt = (uint32_t*)(a + o_ids2);
+    b.node4 = (float4*)(a + o_node4);
+    b.children = (uint2*)(a + o_child);
+    b.parent = (uint32_t*)(a + o_parent);
+    b.aabb = (float4*)(a + o_aabb);
+    b.range = (uint2*)(a + o_range);
+    b.big = (double2*)(a + o_big);
+    b.bound = (uint32_t*)(a + o_bound);
+    b.scratch = (bh::StepScratch*)(a + o_scr);
+    b.status = (uint32_t*)(a + o_status);
+    b.tiles = tiles;
+    b.err = (uint32_t*)(a + o_err);
+    BH_CUDA(s, cudaMemsetAsync(arena, 0, c.off, s->stream));
+    BH_CUDA(s, cudaMemsetAsync(b.bound, 0xFF, sizeof(uint32_t) * ni, s->stream));
+    BH_CUDA(s, cudaStreamSynchronize(s->stream));
+    s->acc_valid = false;
+    return BH_OK;
+}
+
+// ---- step enqueue -----------------------------------------------------------
+
+static bh::WalkParams walk_params(const bh_sim* s, int mode) {
+    const bh_config& c = s->cfg;
+    bh::WalkParams p;
+    p.n = s->b.n;
+    p.g = c.grav_constant;
+    p.theta = c.bh_theta;
+    p.dt = c.delta_time;
+    // (epsMult * sqrt(G m dt))^2 = epsMult^2 G dt m   (barnes_hut.wgsl:90-92)
+    p.eps_coef = c.epsilon_multiplier * c.epsilon_multiplier * c.grav_constant * c.delta_time;
+    p.eps2 = c.plummer_eps * c.plummer_eps;
+    p.plummer = c.softening == BH_SOFTENING_PLUMMER;
+    p.leaf_size = c.leaf_size;
+    p.mode = mode;
+    p.count = 0;
+    p.counters = nullptr;
+    return p;
+}
+
+static bool needs_bbox(const bh_sim* s) {
+    return s->cfg.morton_bits == 64 || s->cfg.morton_domain == BH_DOMAIN_BBOX;
+}
+
+// Tree stages: scratch reset, bbox, Morton encode, sort, build + fill.
+template <class Mark>
+static void enqueue_tree(bh_sim* s, Mark mark) {
+    const DeviceBuffers& b = s->b;
+    cudaStream_t st = s->stream;
+    cudaMemsetAsync(b.scratch, 0, sizeof(bh::StepScratch), st);
+    cudaMemsetAsync(b.status, 0, sizeof(uint32_t) * (size_t)b.key_bytes * b.tiles * bh::kRadix, st);
+    mark(1);
+    if (needs_bbox(s)) bh::launch_bbox(b, st);
+    bh::launch_encode(b, s->cfg.morton_domain, st);
+    mark(2);
+    bh::launch_sort(b, st);
+    mark(3);
+    bh::launch_build_fill(b, s->cfg.fp64_levels, st);
+    mark(4);
+}
+
+// One integration step (simulation.ts:394-420).
+template <class Mark>
+static void enqueue_step(bh_sim* s, Mark mark) {
+    const bool kdk = s->cfg.integrator == BH_INTEGRATOR_LEAPFROG_KDK;
+    mark(0);
+    if (kdk) bh::launch_kick_drift(s->b, s->cfg.delta_time, s->stream);
+    enqueue_tree(s, mark);
+    bh::launch_walk(s->b, walk_params(s, kdk ? bh::kWalkKdkClose : bh::kWalkEulerKickDrift),
+                    s->cfg.walk_block, s->stream);
+    mark(5);
+}
+
+template <class Mark>
+static void enqueue_forces(bh_sim* s, Mark mark) {
+    mark(0);
+    enqueue_tree(s, mark);
+    bh::launch_walk(s->b, walk_params(s, bh::kWalkForces), s->cfg.walk_block, s->stream);
+    mark(5);
+}
+
+static int capture_graph(bh_sim* s, int variant) {
+    cudaStream_t st = s->stream;
+    BH_CUDA(s, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(s, [&](int k) {
+        if (variant == 1) cudaEventRecordWithFlags(s->markers[k], st, cudaEventRecordExternal);
+    });
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (e != cudaSuccess) return cuda_fail(s, e, "cudaStreamEndCapture(step)");
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(s, e, "kernel launch during capture");
+    }
+    if (variant == 1) {
+        size_t count = 0;
+        BH_CUDA(s, cudaGraphGetNodes(g, nullptr, &count));
+        std::vector<cudaGraphNode_t> nodes(count);
+        BH_CUDA(s, cudaGraphGetNodes(g, nodes.data(), &count));
+        for (int k = 0; k < kMarkers; ++k) s->ev_node[k] = nullptr;
+        for (auto nd : nodes) {
+            cudaGraphNodeType t;
+            BH_CUDA(s, cudaGraphNodeGetType(nd, &t));
+            if (t != cudaGraphNodeTypeEventRecord) continue;
+            cudaEvent_t ev;
+            BH_CUDA(s, cudaGraphEventRecordNodeGetEvent(nd, &ev));
+            for (int k = 0; k < kMarkers; ++k)
+                if (ev == s->markers[k]) s->ev_node[k] = nd;
+        }
+        for (int k = 0; k < kMarkers; ++k)
+            if (!s->ev_node[k]) {
+                cudaGraphDestroy(g);
+                return fail(s, BH_ERR_CUDA, "profiling graph lost a stage marker");
+            }
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(s, e, "cudaGraphInstantiate(step)");
+    }
+    s->graph[variant] = g;
+    s->exec[variant] = ex;
+    return BH_OK;
+}
+
+static cudaEvent_t* prof_slot(bh_sim* s) {
+    if (!s->profiling || s->prof_used >= s->prof_max) return nullptr;
+    return &s->prof_ev[(size_t)s->prof_used * kMarkers];
+}
+
+static int check_device_errors(bh_sim* s) {
+    uint32_t e = 0;
+    BH_CUDA(s, cudaMemcpy(&e, s->b.err, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e == 0) return BH_OK;
+    BH_CUDA(s, cudaMemset(s->b.err, 0, sizeof(uint32_t)));
+    std::string msg = "device check failed:";
+    if (e & bh::kErrLookbackSpin) msg += " sort look-back gave up waiting;";
+    if (e & bh::kErrStackOverflow) msg += " walk stack full (children dropped);";
+    if (e & bh::kErrTreeSpin) msg += " tree build gave up waiting;";
+    // Restore the build's exchange slots so the next step starts clean.
+    if (s->b.n > 1) BH_CUDA(s, cudaMemset(s->b.bound, 0xFF, sizeof(uint32_t) * (s->b.n - 1)));
+    return fail(s, BH_ERR_DEVICE_CHECK, msg);
+}
+
+#define BH_HANDLE(s)                                                                        \
+    do {                                                                                    \
+        if (!(s)) return fail(nullptr, BH_ERR_INVALID_ARGUMENT, "null bh_sim handle");      \
+        cudaError_t _d = cudaSetDevice((s)->device);                                        \
+        if (_d != cudaSuccess) return cuda_fail((s), _d, "cudaSetDevice");                  \
+    } while (0)
+
+// ---- lifetime ------------------------------------------------------------------
+
+extern "C" int bh_create(const bh_config* config, bh_sim** out) {
+    if (!out) return fail(nullptr, BH_ERR_INVALID_ARGUMENT, "bh_create: null output");
+    *out = nullptr;
+    bh_sim* s = new bh_sim();
+    if (config) s->cfg = *config;
+    else bh_default_config(&s->cfg);
+    int rc = validate_config(s, s->cfg);
+    if (rc != BH_OK) {
+        delete s;
+        return rc;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        delete s;
+        return fail(nullptr, BH_ERR_NO_DEVICE,
+                    std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "0 devices"));
+    }
+    if (s->cfg.device < 0 || s->cfg.device >= ndev) {
+        delete s;
+        return fail(nullptr, BH_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    }
+    s->device = s->cfg.device;
+    if ((e = cudaSetDevice(s->device)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = bh::sort_init_attributes()) != cudaSuccess) {
+        int r = cuda_fail(nullptr, e, "bh_create");
+        delete s;
+        return r;
+    }
+    for (int k = 0; k < kMarkers; ++k) cudaEventCreate(&s->markers[k]);
+    rc = alloc_buffers(s, s->n);
+    if (rc != BH_OK) {
+        std::string m = s->err;
+        bh_destroy(s);
+        return fail(nullptr, rc, m);
+    }
+    *out = s;
+    return BH_OK;
+}
+
+static void free_profile(bh_sim* s) {
+    for (auto ev : s->prof_ev) cudaEventDestroy(ev);
+    s->prof_ev.clear();
+    s->profiling = false;
+    s->prof_max = s->prof_used = 0;
+}
+
+extern "C" int bh_destroy(bh_sim* s) {
+    if (!s) return BH_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    free_buffers(s);
+    free_profile(s);
+    for (int k = 0; k < kMarkers; ++k)
+        if (s->markers[k]) cudaEventDestroy(s->markers[k]);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return BH_OK;
+}
+
+extern "C" int bh_generate_scenario(const char* name, uint32_t n, uint64_t seed,
+                                    float grav_constant, float* mass, float* pos, float* vel,
+                                    float* radius_multiplier) {
+    if (!name) return fail(nullptr, BH_ERR_INVALID_ARGUMENT, "null scenario name");
+    if (n > 0 && (!mass || !pos || !vel))
+        return fail(nullptr, BH_ERR_INVALID_ARGUMENT, "null output array");
+    if (bh::generate_scenario(name, n, seed, grav_constant, mass, pos, vel, radius_multiplier) != 0)
+        return fail(nullptr, BH_ERR_UNKNOWN_SCENARIO, std::string("Unknown scenario: ") + name);
+    return BH_OK;
+}
+
+static int load_scenario(bh_sim* s, const std::string& name, uint64_t seed, uint32_t n) {
+    std::vector<float> mass(n), pos(2 * (size_t)n), vel(2 * (size_t)n), rad(n);
+    if (bh::generate_scenario(name.c_str(), n, seed, s->cfg.grav_constant, mass.data(), pos.data(),
+                              vel.data(), rad.data()) != 0)
+        return fail(s, BH_ERR_UNKNOWN_SCENARIO, "Unknown scenario: " + name);
+    // New buffers on every scenario change (simulation.ts:367-369).
+    int rc = alloc_buffers(s, n);
+    if (rc != BH_OK) return rc;
+    s->scenario = name;
+    s->seed = seed;
+    s->n = n;
+    if (n) {
+        BH_CUDA(s, cudaMemcpyAsync(s->b.mass, mass.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+        BH_CUDA(s, cudaMemcpyAsync(s->b.pos, pos.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+        BH_CUDA(s, cudaMemcpyAsync(s->b.vel, vel.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+        BH_CUDA(s, cudaMemcpyAsync(s->b.radius, rad.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    }
+    BH_CUDA(s, cudaStreamSynchronize(s->stream));
+    return BH_OK;
+}
+
+extern "C" int bh_set_num_bodies(bh_sim* s, uint32_t n) {
+    BH_HANDLE(s);
+    if (n > kMaxBodies) return fail(s, BH_ERR_INVALID_ARGUMENT, "body count above 2^30 - 1");
+    return load_scenario(s, s->scenario, s->seed, n);  // simulation.ts:227-231
+}
+
+extern "C" int bh_set_scenario(bh_sim* s, const char* name, uint64_t seed) {
+    BH_HANDLE(s);
+    if (!name) return fail(s, BH_ERR_INVALID_ARGUMENT, "null scenario name");
+    return load_scenario(s, name, seed, s->n);
+}
+
+extern "C" int bh_update_metadata(bh_sim* s) {
+    BH_HANDLE(s);
+    return validate_config(s, s->cfg);
+}
+
+extern "C" int bh_upload(bh_sim* s, const float* mass, const float* pos, const float* vel, uint32_t n) {
+    BH_HANDLE(s);
+    if (n != s->b.n) return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_upload: n differs from the body count");
+    if (n == 0) return BH_OK;
+    if (mass) BH_CUDA(s, cudaMemcpyAsync(s->b.mass, mass, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    if (pos) BH_CUDA(s, cudaMemcpyAsync(s->b.pos, pos, 8 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    if (vel) BH_CUDA(s, cudaMemcpyAsync(s->b.vel, vel, 8 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    if (mass || pos) s->acc_valid = false;
+    return BH_OK;
+}
+
+extern "C" int bh_download(bh_sim* s, float* mass, float* pos, float* vel, uint32_t n) {
+    BH_HANDLE(s);
+    if (n != s->b.n) return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_download: n differs from the body count");
+    if (n) {
+        if (mass) BH_CUDA(s, cudaMemcpyAsync(mass, s->b.mass, 4 * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
+        if (pos) BH_CUDA(s, cudaMemcpyAsync(pos, s->b.pos, 8 * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
+        if (vel) BH_CUDA(s, cudaMemcpyAsync(vel, s->b.vel, 8 * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
+    }
+    BH_CUDA(s, cudaStreamSynchronize(s->stream));
+    return check_device_errors(s);
+}
+
+// ---- stepping --------------------------------------------------------------------
+
+static int step_once(bh_sim* s) {
+    const bool kdk = s->cfg.integrator == BH_INTEGRATOR_LEAPFROG_KDK;
+    if (kdk && !s->acc_valid) {
+        enqueue_forces(s, [](int) {});  // first force evaluation of a leapfrog run
+        s->acc_valid = true;
+    }
+    cudaEvent_t* ev = prof_slot(s);
+    if (s->cfg.use_graphs) {
+        const int v = ev ? 1 : 0;
+        if (!s->exec[v]) {
+            int rc = capture_graph(s, v);
+            if (rc != BH_OK) return rc;
+        }
+        if (ev)
+            for (int k = 0; k < kMarkers; ++k)
+                BH_CUDA(s, cudaGraphExecEventRecordNodeSetEvent(s->exec[1], s->ev_node[k], ev[k]));
+        BH_CUDA(s, cudaGraphLaunch(s->exec[v], s->stream));
+    } else {
+        enqueue_step(s, [&](int k) {
+            if (ev) cudaEventRecord(ev[k], s->stream);
+        });
+        BH_CUDA(s, cudaGetLastError());
+    }
+    if (ev) s->prof_used++;
+    s->acc_valid = kdk;
+    return BH_OK;
+}
+
+extern "C" int bh_step(bh_sim* s, uint32_t frames) {
+    BH_HANDLE(s);
+    if (s->b.n == 0) return BH_OK;
+    const uint64_t steps = (uint64_t)frames * (uint64_t)s->cfg.substeps;  // simulation.ts:393
+    for (uint64_t i = 0; i < steps; ++i) {
+        int rc = step_once(s);
+        if (rc != BH_OK) return rc;
+    }
+    return BH_OK;
+}
+
+extern "C" int bh_sync(bh_sim* s) {
+    BH_HANDLE(s);
+    BH_CUDA(s, cudaStreamSynchronize(s->stream));
+    return check_device_errors(s);
+}
+
+extern "C" int bh_compute_accelerations(bh_sim* s, float* acc_host) {
+    BH_HANDLE(s);
+    if (s->b.n == 0) return BH_OK;
+    enqueue_forces(s, [](int) {});
+    BH_CUDA(s, cudaGetLastError());
+    if (acc_host)
+        BH_CUDA(s, cudaMemcpyAsync(acc_host, s->b.acc, 8 * (size_t)s->b.n, cudaMemcpyDeviceToHost, s->stream));
+    BH_CUDA(s, cudaStreamSynchronize(s->stream));
+    s->acc_valid = true;
+    return check_device_errors(s);
+}
+
+extern "C" int bh_walk_stats(bh_sim* s, uint64_t* node_visits, uint64_t* interactions) {
+    BH_HANDLE(s);
+    unsigned long long h[2] = {0, 0};
+    if (s->b.n > 0) {
+        enqueue_tree(s, [](int) {});
+        bh::WalkParams p = walk_params(s, bh::kWalkForces);
+        p.count = 1;
+        p.counters = s->b.scratch->walk_counts;
+        bh::launch_walk(s->b, p, s->cfg.walk_block, s->stream);
+        BH_CUDA(s, cudaGetLastError());
+        BH_CUDA(s, cudaMemcpyAsync(h, s->b.scratch->walk_counts, sizeof(h), cudaMemcpyDeviceToHost,
+                                   s->stream));
+        BH_CUDA(s, cudaStreamSynchronize(s->stream));
+        s->acc_valid = true;
+    }
+    if (node_visits) *node_visits = h[0];
+    if (interactions) *interactions = h[1];
+    return check_device_errors(s);
+}
+
+// ---- buffers -----------------------------------------------------------------------
+
+extern "C" int bh_get_buffers(bh_sim* s, bh_buffers* out) {
+    BH_HANDLE(s);
+    if (!out) return fail(s, BH_ERR_INVALID_ARGUMENT, "null output");
+    const DeviceBuffers& b = s->b;
+    out->mass = b.mass;
+    out->pos = (float*)b.pos;
+    out->vel = (float*)b.vel;
+    out->radius_multiplier = b.radius;
+    out->acc = (float*)b.acc;
+    out->morton_codes = b.codes;
+    out->body_indices = b.ids;
+    out->node4 = (float*)b.node4;
+    out->node_children = (uint32_t*)b.children;
+    out->node_parent = b.parent;
+    out->node_aabb = (float*)b.aabb;
+    out->num_bodies = b.n;
+    out->morton_bits = s->cfg.morton_bits;
+    out->stream = (void*)s->stream;
+    return BH_OK;
+}
+
+extern "C" int bh_get_num_bodies(bh_sim* s, uint32_t* out) {
+    if (!s || !out) return fail(s, BH_ERR_INVALID_ARGUMENT, "null argument");
+    *out = s->b.n;
+    return BH_OK;
+}
+
+extern "C" int bh_read_buffer(bh_sim* s, const char* name, void* host, size_t bytes) {
+    BH_HANDLE(s);
+    if (!name || (!host && bytes)) return fail(s, BH_ERR_INVALID_ARGUMENT, "null argument");
+    const DeviceBuffers& b = s->b;
+    const size_t n = b.n, nn = n ? 2 * n - 1 : 0, ni = n > 1 ? n - 1 : 0;
+    const std::string nm(name);
+    const void* src = nullptr;
+    size_t cap = 0;
+    if (nm == "mass") { src = b.mass; cap = 4 * n; }
+    else if (nm == "pos") { src = b.pos; cap = 8 * n; }
+    else if (nm == "vel") { src = b.vel; cap = 8 * n; }
+    else if (nm == "acc") { src = b.acc; cap = 8 * n; }
+    else if (nm == "radius_multiplier") { src = b.radius; cap = 4 * n; }
+    else if (nm == "morton_codes") { src = b.codes; cap = (size_t)b.key_bytes * n; }
+    else if (nm == "body_indices") { src = b.ids; cap = 4 * n; }
+    else if (nm == "node4") { src = b.node4; cap = 16 * nn; }
+    else if (nm == "node_children") { src = b.children; cap = 8 * ni; }
+    else if (nm == "node_parent") { src = b.parent; cap = 4 * nn; }
+    else if (nm == "node_aabb") { src = b.aabb; cap = 16 * ni; }
+    else return fail(s, BH_ERR_INVALID_ARGUMENT, "unknown buffer name: " + nm);
+    if (bytes > cap) return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_read_buffer: size above the buffer");
+    BH_CUDA(s, cudaStreamSynchronize(s->stream));
+    if (bytes) BH_CUDA(s, cudaMemcpy(host, src, bytes, cudaMemcpyDeviceToHost));
+    return BH_OK;
+}
+
+// ---- profiling -----------------------------------------------------------------------
+
+extern "C" int bh_profile_begin(bh_sim* s, uint32_t max_steps) {
+    BH_HANDLE(s);
+    if (max_steps == 0 || max_steps > 100000)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "max_steps must be in [1, 100000]");
+    free_profile(s);
+    s->prof_ev.resize((size_t)max_steps * kMarkers);
+    for (auto& ev : s->prof_ev) BH_CUDA(s, cudaEventCreate(&ev));
+    s->prof_max = max_steps;
+    s->prof_used = 0;
+    s->profiling = true;
+    return BH_OK;
+}
+
+extern "C" int bh_profile_end(bh_sim* s, double* stage_ms, uint32_t* steps_recorded) {
+    BH_HANDLE(s);
+    if (!s->profiling) return fail(s, BH_ERR_INVALID_ARGUMENT, "profiling was not started");
+    BH_CUDA(s, cudaStreamSynchronize(s->stream));
+    double acc[BH_NUM_STAGES] = {0, 0, 0, 0, 0};
+    // marker k -> stage: [0,1] other, [1,2] morton, [2,3] sort, [3,4] tree, [4,5] walk
+    const int stage_of[5] = {BH_STAGE_OTHER, BH_STAGE_MORTON, BH_STAGE_SORT, BH_STAGE_TREE, BH_STAGE_WALK};
+    for (uint32_t i = 0; i < s->prof_used; ++i) {
+        cudaEvent_t* ev = &s->prof_ev[(size_t)i * kMarkers];
+        for (int k = 0; k < 5; ++k) {
+            float ms = 0.f;
+            BH_CUDA(s, cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+            acc[stage_of[k]] += ms;
+        }
+    }
+    if (stage_ms)
+        for (int k = 0; k < BH_NUM_STAGES; ++k) stage_ms[k] = acc[k];
+    if (steps_recorded) *steps_recorded = s->prof_used;
+    free_profile(s);
+    return check_device_errors(s);
+}
+
+extern "C" int bh_kernels_per_step(bh_sim* s, uint32_t* out) {
+    if (!s || !out) return fail(s, BH_ERR_INVALID_ARGUMENT, "null argument");
+    uint32_t k = 0;
+    if (s->cfg.integrator == BH_INTEGRATOR_LEAPFROG_KDK) k += 1;  // kick + drift
+    if (needs_bbox(s)) k += 1;                                      // bbox
+    k += 1;                                                         // encode
+    k += (uint32_t)bh::sort_passes(s->b);                          // sort passes
+    k += 1;                                                         // build + fill
+    k += 1;                                                         // walk + integrate
+    *out = s->b.n ? k : 0;
+    return BH_OK;
+}
+
+// ---- errors ----------------------------------------------------------------------------
+
+extern "C" const char* bh_last_error(bh_sim* s) { return s ? s->err.c_str() : g_err.c_str(); }
+extern "C" const char* bh_global_last_error(void) { return g_err.c_str(); }
+extern "C" const char* bh_version(void) { return "bh-b200 0.1.0 (sm_100a)"; }
