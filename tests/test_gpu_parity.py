@@ -165,6 +165,11 @@ def test_profile_and_kernel_count(bh):
     assert steps == 5
     assert all(v >= 0 for v in ms.values()) and ms["walk"] > 0
     assert sim.kernels_per_step() == 1 + 4 + 1 + 1  # encode, 4 sort passes, build+fill, walk
+    # a second profiling window on the same captured graph
+    sim.profile_begin(3)
+    sim.step(3)
+    ms2, steps2 = sim.profile_end()
+    assert steps2 == 3 and ms2["walk"] > 0
     sim.close()
 
 

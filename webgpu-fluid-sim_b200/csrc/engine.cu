@@ -371,6 +371,13 @@ extern "C" int bh_create(const bh_config* config, bh_sim** out) {
 }
 
 static void free_profile(bh_sim* s) {
+    // The profiled graph's event nodes may still name events of this pool:
+    // point them back at the persistent markers before the pool goes away.
+    if (s->exec[1] && !s->prof_ev.empty()) {
+        cudaStreamSynchronize(s->stream);
+        for (int k = 0; k < kMarkers; ++k)
+            if (s->ev_node[k]) cudaGraphExecEventRecordNodeSetEvent(s->exec[1], s->ev_node[k], s->markers[k]);
+    }
     for (auto ev : s->prof_ev) cudaEventDestroy(ev);
     s->prof_ev.clear();
     s->profiling = false;
