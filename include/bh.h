@@ -184,6 +184,30 @@ int bh_kernels_per_step(bh_sim* sim, uint32_t* out);
  * forces; does not integrate. */
 int bh_walk_stats(bh_sim* sim, uint64_t* node_visits, uint64_t* interactions);
 
+/* ---- allocation-free hierarchy build ------------------------------------ */
+/* No counterpart in the reference.  For callers that cannot let this library
+ * allocate device memory (a host that plans the whole GPU heap and hands out
+ * every buffer, a frame loop that cannot take the device-wide sync of
+ * cudaMalloc/cudaFree, code that must not allocate once running): builds the
+ * hierarchy and fills node mass/COM/AABB -- the same kernel and results as the
+ * tree stage of bh_step -- from caller-owned device buffers, with the
+ * kernel's scratch in a static device array inside the library.
+ *   in : sorted_codes[n] (uint32, or uint64 when morton_bits == 64),
+ *        sorted_ids[n], mass[n], pos[2n] (original body order)
+ *   out: node4[4(2n-1)], node_children[2(n-1)], node_parent[2n-1],
+ *        node_aabb[4(n-1)]  (layouts as in bh_buffers)
+ * Limit: n <= 262144 (larger n returns BH_ERR_INVALID_ARGUMENT).  Enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream); calls no cudaMalloc
+ * or cudaFree.  All calls share the static scratch: calls that overlap on the
+ * GPU race, so serialise them.  The first call on a device looks the scratch
+ * up with cudaGetSymbolAddress; make it before any stream capture.  Errors are
+ * reported through bh_global_last_error(). */
+int bh_build_hierarchy_static(const void* sorted_codes, int32_t morton_bits,
+                              const uint32_t* sorted_ids, const float* mass, const float* pos,
+                              uint32_t n, float* node4, uint32_t* node_children,
+                              uint32_t* node_parent, float* node_aabb, int32_t fp64_levels,
+                              void* stream);
+
 /* ---- errors ------------------------------------------------------------- */
 const char* bh_last_error(bh_sim* sim);
 const char* bh_global_last_error(void);

@@ -95,6 +95,8 @@ SIGNATURES = {
     "bh_kernels_per_step": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint32)]),
     "bh_walk_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_uint64)]),
+    "bh_build_hierarchy_static": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _P, ctypes.c_uint32,
+                                                 _P, _P, _P, _P, ctypes.c_int32, _P]),
     "bh_last_error": (ctypes.c_char_p, [_P]),
     "bh_global_last_error": (ctypes.c_char_p, []),
     "bh_version": (ctypes.c_char_p, []),

@@ -49,6 +49,11 @@ struct bh_sim {
 
 static thread_local std::string g_err;
 
+namespace bh {
+// Message for bh_global_last_error() from entry points without a handle.
+void set_global_error(const std::string& msg) { g_err = msg; }
+}  // namespace bh
+
 static int fail(bh_sim* s, int code, const std::string& msg) {
     if (s) s->err = msg;
     g_err = msg;

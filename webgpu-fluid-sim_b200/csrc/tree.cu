@@ -1,154 +1,8 @@
-// tree.cu -- hierarchy build and mass / centre-of-mass / AABB fill in one
-// bottom-up pass.
-//
-// Reference: build_lbvh_main (lbvh.wgsl:85-165, Karras 2012 fig. 4) followed by
-// fill_lbvh_main (lbvh.wgsl:168-232).  The reference builds top-down with one
-// thread per internal node and binary searches, then climbs from the leaves
-// with arrival counters but no memory fences, which its README calls a race.
-//
-// Here one thread per sorted slot climbs from its leaf and creates each
-// internal node when it is the second child to arrive (agglomerative build,
-// Apetrei 2014), using the same delta(i, j) as lbvh.wgsl:72-83:
-//   delta = clz(k_i ^ k_j), or key_bits + clz(i ^ j) for equal keys, -1 outside.
-// A node covering sorted slots [l, r] is the left child of its parent when
-// delta(r, r+1) > delta(l-1, l), and the parent's split is then r; otherwise it
-// is the right child and the split is l-1.  Karras numbers an internal node by
-// the end of its range next to its parent's split (a left child by its last
-// slot, a right child by its first slot, the root is 0), and its children are
-// gamma / gamma+1, or the leaves n-1+gamma / n+gamma when a side holds one slot
-// (lbvh.wgsl:141-152).  Computing those indices here gives the same
-// left/right/parent arrays as the reference's top-down build, bit for bit.
-//
-// Synchronisation: the two children of a split gamma meet at bound[gamma] with
-// an atomic exchange of their far range ends; the first arriver stops.  Node
-// records are published with __threadfence() before the exchange and read by
-// the second arriver through L2 (__ldcg) after it, so no stale data is ever
-// combined.  There are no spins.  bound[] holds kSentinel between steps: the
-// second arriver restores it.
-//
-// Mass / COM: small nodes use the reference's f32 formula
-//   M = m_l + m_r;  com = (c_l m_l + c_r m_r) / M  (0 if M <= 0)   (lbvh.wgsl:216-224)
-// and nodes of >= kFp64MinBodies bodies aggregate {m, m x, m y} in FP64.
-// AABB and length = longest side are exact (lbvh.wgsl:212-213,227-228).
-#include "bh_internal.cuh"
+// tree.cu -- launches the fused hierarchy build + fill for the engine's step.
+// The kernel and its derivation are in tree_kernel.cuh.
+#include "tree_kernel.cuh"
 
 namespace bh {
-
-template <typename K>
-__device__ __forceinline__ int delta_at(const K* __restrict__ keys, uint32_t i, uint32_t j) {
-    K a = __ldg(&keys[i]), b = __ldg(&keys[j]);
-    if (a == b) return (int)(8 * sizeof(K)) + __clz((int)(i ^ j));
-    if (sizeof(K) == 8) return __clzll((long long)(a ^ b));
-    return __clz((int)(uint32_t)(a ^ b));
-}
-
-template <typename K>
-__global__ void __launch_bounds__(256)
-build_fill_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ ids,
-                  const float* __restrict__ mass, const float2* __restrict__ pos,
-                  float4* __restrict__ node4, uint2* __restrict__ children,
-                  uint32_t* __restrict__ parent, float4* __restrict__ aabb,
-                  uint2* __restrict__ range, double2* __restrict__ big,
-                  uint32_t* __restrict__ bound, uint32_t n, int fp64) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t nm1 = n - 1;
-    const uint32_t body = __ldg(&ids[i]);
-    const float m = __ldg(&mass[body]);
-    const float2 p = __ldg(&pos[body]);
-    node4[nm1 + i] = make_float4(p.x, p.y, m, 0.0f);  // leaf (lbvh.wgsl:179-187)
-    if (n == 1) {
-        parent[0] = kSentinel;
-        return;
-    }
-    // Running record of the node this thread currently owns.
-    float cm = m, cx = p.x, cy = p.y;
-    float lox = p.x, loy = p.y, hix = p.x, hiy = p.y;
-    double dm = 0.0, dmx = 0.0, dmy = 0.0;  // valid when the node has >= kFp64MinBodies bodies
-    uint32_t l = i, r = i;
-    while (true) {
-        const int dl = (l == 0) ? -1 : delta_at(keys, l - 1, l);
-        const int dr = (r == nm1) ? -1 : delta_at(keys, r, r + 1);
-        const bool is_left = dr > dl;
-        const uint32_t gamma = is_left ? r : l - 1;
-        __threadfence();
-        const uint32_t other = atomicExch(&bound[gamma], is_left ? l : r);
-        if (other == kSentinel) return;  // first to arrive: the sibling finishes the parent
-        __threadfence();
-        bound[gamma] = kSentinel;
-        const uint32_t pl = is_left ? l : other;
-        const uint32_t pr = is_left ? other : r;
-        const uint32_t li = (pl == gamma) ? nm1 + gamma : gamma;
-        const uint32_t ri = (pr == gamma + 1) ? nm1 + gamma + 1 : gamma + 1;
-        const uint32_t sib = is_left ? ri : li;
-        const uint32_t sib_cnt = is_left ? (pr - gamma) : (gamma - pl + 1);
-        const uint32_t my_cnt = r - l + 1;
-        const float4 s4 = __ldcg(&node4[sib]);
-        const float4 sb = (sib >= nm1) ? make_float4(s4.x, s4.y, s4.x, s4.y) : __ldcg(&aabb[sib]);
-        lox = fminf(lox, sb.x);
-        loy = fminf(loy, sb.y);
-        hix = fmaxf(hix, sb.z);
-        hiy = fmaxf(hiy, sb.w);
-        const uint32_t cnt = pr - pl + 1;
-        // Parent's own Karras index.
-        uint32_t pidx;
-        if (pl == 0 && pr == nm1) {
-            pidx = 0;
-        } else {
-            const int dpl = (pl == 0) ? -1 : delta_at(keys, pl - 1, pl);
-            const int dpr = (pr == nm1) ? -1 : delta_at(keys, pr, pr + 1);
-            pidx = (dpr > dpl) ? pr : pl;
-        }
-        float tm, ncx, ncy;
-        if (fp64 && cnt >= kFp64MinBodies) {
-            double sm, smx, smy;
-            if (sib_cnt >= kFp64MinBodies) {
-                const double2 s0 = __ldcg(&big[2 * (size_t)sib]);
-                const double2 s1 = __ldcg(&big[2 * (size_t)sib + 1]);
-                sm = s0.x; smx = s0.y; smy = s1.x;
-            } else {
-                sm = (double)s4.z; smx = (double)s4.z * (double)s4.x; smy = (double)s4.z * (double)s4.y;
-            }
-            if (my_cnt < kFp64MinBodies) {
-                dm = (double)cm; dmx = (double)cm * (double)cx; dmy = (double)cm * (double)cy;
-            }
-            dm += sm;
-            dmx += smx;
-            dmy += smy;
-            tm = (float)dm;
-            ncx = dm > 0.0 ? (float)(dmx / dm) : 0.0f;
-            ncy = dm > 0.0 ? (float)(dmy / dm) : 0.0f;
-            big[2 * (size_t)pidx] = make_double2(dm, dmx);
-            big[2 * (size_t)pidx + 1] = make_double2(dmy, 0.0);
-        } else {
-            float ml, mr, clx, cly, crx, cry;
-            if (is_left) { ml = cm; clx = cx; cly = cy; mr = s4.z; crx = s4.x; cry = s4.y; }
-            else { ml = s4.z; clx = s4.x; cly = s4.y; mr = cm; crx = cx; cry = cy; }
-            tm = __fadd_rn(ml, mr);
-            if (tm > 0.0f) {
-                ncx = __fdiv_rn(__fadd_rn(__fmul_rn(clx, ml), __fmul_rn(crx, mr)), tm);
-                ncy = __fdiv_rn(__fadd_rn(__fmul_rn(cly, ml), __fmul_rn(cry, mr)), tm);
-            } else {
-                ncx = 0.0f;
-                ncy = 0.0f;
-            }
-        }
-        const float len = fmaxf(__fsub_rn(hix, lox), __fsub_rn(hiy, loy));
-        node4[pidx] = make_float4(ncx, ncy, tm, len);
-        aabb[pidx] = make_float4(lox, loy, hix, hiy);
-        children[pidx] = make_uint2(li, ri);
-        range[pidx] = make_uint2(pl, pr);
-        parent[li] = pidx;
-        parent[ri] = pidx;
-        if (pidx == 0) {
-            parent[0] = kSentinel;  // lbvh.wgsl:159-161
-            return;
-        }
-        cm = tm; cx = ncx; cy = ncy;
-        l = pl;
-        r = pr;
-    }
-}
 
 void init_bound(const DeviceBuffers& b, cudaStream_t s) {
     if (b.n > 1) cudaMemsetAsync(b.bound, 0xFF, sizeof(uint32_t) * (b.n - 1), s);
