@@ -156,7 +156,8 @@ def cpu_baseline(pkg, wl, seconds_budget=20.0):
             break
     return {"value": n * steps / el, "unit": "body-steps/s", "cores": threads, "kind": "port",
             "sample": f"{steps} steps of the full {n}-body workload after 1 warm-up step "
-                      f"(oracle: reference per-body monopole walk, {threads} OpenMP threads)"}
+                      f"(oracle C restatement, same algorithm as the engine: {cfg.walk} walk, "
+                      f"{threads} OpenMP threads)"}
 
 
 # ---------------------------------------------------------------- reference arm
@@ -249,7 +250,7 @@ def run_own(args):
     value = world * n * K / (step_ms_max / 1e3)
 
     # ---- walk statistics + force error (untimed) ----
-    visits, interactions = sim.walk_stats()
+    visits, multi_inter, body_inter = sim.walk_stats()
     mass, pos, vel = sim.download()
     acc = sim.read_buffer("acc", np.float32, 2 * n).reshape(n, 2)
     med_err, p99_err, nsamp = force_error_vs_fp64(acc, mass, pos, cfg)
@@ -288,10 +289,15 @@ def run_own(args):
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         except OSError:
             pass
-        # dominant kernel: the walk.  Algorithmic flops per launch = 16 FP32
-        # flops per interaction (monopole walk) x interactions of the step.
+        # dominant kernel: the walk.  Algorithmic FP32 flops per launch:
+        # 16 per monopole interaction (2 sub, 3 for d^2+eps^2, 4 for rsqrt,
+        # 2 for inv^3, 1 for m inv^3, 4 for two FMA) and 35 per
+        # monopole + quadrupole interaction (the 16 plus Q'r 6, r.Q'r 3,
+        # inv^5 1, 2.5 r.Q'r inv^7 3, two extra FMA 4, one add 2) x the
+        # interactions counted by an instrumented launch of the same walk.
         walk_ms = stage_ms["walk"] / max(recorded, 1)
-        flops = 16.0 * interactions
+        quad = cfg.walk == "group" and cfg.multipole >= 2
+        flops = (35.0 if quad else 16.0) * multi_inter + 16.0 * body_inter
         sm_mhz = clk.get("sm_max_mhz") or 1965.0
         fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # nominal FMA peak at max clock
         achieved = flops / (walk_ms / 1e3) / 1e12
@@ -299,8 +305,11 @@ def run_own(args):
                     "frac": achieved / fp32_peak, "traffic": None,
                     "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2 x max SM clock);"
                                    " no measured FP32 peak exists for this pool",
-                    "kernel": "walk", "kernel_ms": walk_ms, "interactions_per_step": interactions,
-                    "node_visits_per_step": visits}
+                    "kernel": "walk", "kernel_ms": walk_ms,
+                    "multipole_interactions_per_step": multi_inter,
+                    "body_interactions_per_step": body_inter,
+                    "node_visits_per_step": visits,
+                    "flops_per_step": flops}
         stages = {k: v / max(recorded, 1) for k, v in stage_ms.items()}
         hbm = peaks.get("hbm_gbs", 6650.0)
         kps = sim.kernels_per_step()

@@ -68,8 +68,14 @@ typedef struct bh_config {
     int32_t device;           /* CUDA device ordinal */
     int32_t use_graphs;       /* 1 = replay each step from a captured CUDA graph */
     int32_t fp64_levels;      /* 1 = FP64 mass/COM aggregation for nodes of >= 1024 bodies */
-    int32_t reserved[7];
+    int32_t walk_mode;        /* BH_WALK_EXACT (reference per-body walk) or BH_WALK_GROUP */
+    int32_t multipole_order;  /* group walk: 1 = monopole, 2 = monopole + quadrupole */
+    int32_t bodies_per_lane;  /* group walk: 1, 2 or 4 (group = 32 x this many bodies); 0 = 2 */
+    int32_t reserved[4];
 } bh_config;
+
+#define BH_WALK_EXACT 0 /* lane-exact replica of barnes_hut.wgsl:48-111 (monopole, per-body theta test) */
+#define BH_WALK_GROUP 1 /* extension: per-warp group test (group box vs node box) + multipoles */
 
 /* getDefaultConfig() (config.ts:9-22) plus extension defaults that keep the
  * reference behaviour (reference softening, fixed domain, 32-bit keys,
@@ -179,10 +185,12 @@ int bh_profile_end(bh_sim* sim, double* stage_ms, uint32_t* steps_recorded);
 int bh_kernels_per_step(bh_sim* sim, uint32_t* out);
 
 /* Build the tree at the current positions and run an instrumented force walk
- * that counts, over all bodies, the nodes each body's walk visits and the
- * interactions it evaluates (for rooflines).  Leaves acc[] holding the
- * forces; does not integrate. */
-int bh_walk_stats(bh_sim* sim, uint64_t* node_visits, uint64_t* interactions);
+ * that counts node visits (exact walk: per body; group walk: per group) and
+ * the interactions evaluated over all bodies: with a node's multipole
+ * (monopole, or monopole + quadrupole) and with single bodies (for
+ * rooflines).  Leaves acc[] holding the forces; does not integrate. */
+int bh_walk_stats(bh_sim* sim, uint64_t* node_visits, uint64_t* multipole_interactions,
+                  uint64_t* body_interactions);
 
 /* ---- allocation-free hierarchy build ------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot let this library

@@ -425,6 +425,187 @@ void orc_walk_counts(const orc_params* p, uint32_t n, const uint32_t* ids, const
 }
 
 /* ------------------------------------------------------------------------ */
+/* Extension: quadrupole moments and the group walk                          */
+/* ------------------------------------------------------------------------ */
+
+void orc_quadrupoles(uint32_t n, const uint32_t* left, const uint32_t* right, const float* com,
+                     const float* mass_node, float* quad) {
+    const size_t nn = n ? 2 * (size_t)n - 1 : 0;
+    memset(quad, 0, sizeof(float) * 3 * nn);
+    if (n < 2) return;
+    const uint32_t nm1 = n - 1;
+    uint32_t* st = (uint32_t*)malloc(sizeof(uint32_t) * 2 * (size_t)n);
+    uint8_t* seen = (uint8_t*)calloc(n, 1);
+    int64_t sp = 0;
+    st[sp++] = 0;
+    while (sp > 0) {
+        uint32_t v = st[sp - 1];
+        if (v >= nm1) { sp--; continue; }
+        if (!seen[v]) {
+            seen[v] = 1;
+            st[sp++] = left[v];
+            st[sp++] = right[v];
+            continue;
+        }
+        sp--;
+        const uint32_t l = left[v], r = right[v];
+        const float cx = com[2 * v], cy = com[2 * v + 1];
+        const float ml = mass_node[l], mr = mass_node[r];
+        const float dlx = com[2 * l] - cx, dly = com[2 * l + 1] - cy;
+        const float drx = com[2 * r] - cx, dry = com[2 * r + 1] - cy;
+        quad[3 * v] = (quad[3 * l] + ml * (dlx * dlx)) + (quad[3 * r] + mr * (drx * drx));
+        quad[3 * v + 1] = (quad[3 * l + 1] + ml * (dlx * dly)) + (quad[3 * r + 1] + mr * (drx * dry));
+        quad[3 * v + 2] = (quad[3 * l + 2] + ml * (dly * dly)) + (quad[3 * r + 2] + mr * (dry * dry));
+    }
+    free(st);
+    free(seen);
+}
+
+void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const float* mass,
+                    const float* pos, const float* com, const float* mass_node, const float* aabb,
+                    const float* quad, const uint32_t* left, const uint32_t* right, float* acc) {
+    if (n == 0) return;
+    const uint32_t nm1 = n - 1;
+    const uint32_t G = 32u * (uint32_t)(p->bodies_per_lane > 0 ? p->bodies_per_lane : 2);
+    const uint32_t L = (uint32_t)(p->leaf_size > 1 ? p->leaf_size : 1);
+    const float th2 = p->bh_theta * p->bh_theta;
+    const int plummer = p->softening == ORC_SOFT_PLUMMER;
+    const float eps2 = p->plummer_eps * p->plummer_eps;
+    const float ecoef = p->epsilon_multiplier * p->epsilon_multiplier * p->grav_constant * p->delta_time;
+    uint32_t* first = (uint32_t*)malloc(sizeof(uint32_t) * (2 * (size_t)n - 1));
+    uint32_t* last = (uint32_t*)malloc(sizeof(uint32_t) * (2 * (size_t)n - 1));
+    node_ranges(n, left, right, first, last);
+    /* Groups: maximal subtrees of <= G bodies (contiguous slots of one cell). */
+    uint32_t* gfirst = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* gcount = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t ngroups = 0;
+    {
+        uint32_t* st = (uint32_t*)malloc(sizeof(uint32_t) * 2 * (size_t)n);
+        int64_t sp = 0;
+        st[sp++] = n > 1 ? 0u : nm1;
+        while (sp > 0) {
+            const uint32_t v = st[--sp];
+            const uint32_t c = last[v] - first[v] + 1;
+            if (c <= G) {
+                gfirst[ngroups] = first[v];
+                gcount[ngroups++] = c;
+            } else {
+                st[sp++] = right[v];
+                st[sp++] = left[v];
+            }
+        }
+        free(st);
+    }
+#pragma omp parallel num_threads(nthreads(p))
+    {
+        /* Per-thread lists; a list never holds more than 2n-1 entries, so
+         * capacity 2n can always hold a push. */
+        size_t cap = 4096 < 2 * (size_t)n ? 4096 : 2 * (size_t)n;
+        uint32_t* stack = (uint32_t*)malloc(sizeof(uint32_t) * cap);
+        uint32_t* nodes = (uint32_t*)malloc(sizeof(uint32_t) * cap);
+        uint32_t* rfirst = (uint32_t*)malloc(sizeof(uint32_t) * cap);
+        uint32_t* rcount = (uint32_t*)malloc(sizeof(uint32_t) * cap);
+#define ORC_GROW(need)                                                         \
+        if ((size_t)(need) > cap) {                                            \
+            cap = 2 * cap > (size_t)(need) ? 2 * cap : (size_t)(need);         \
+            stack = (uint32_t*)realloc(stack, sizeof(uint32_t) * cap);         \
+            nodes = (uint32_t*)realloc(nodes, sizeof(uint32_t) * cap);         \
+            rfirst = (uint32_t*)realloc(rfirst, sizeof(uint32_t) * cap);       \
+            rcount = (uint32_t*)realloc(rcount, sizeof(uint32_t) * cap);       \
+        }
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t g = 0; g < (int64_t)ngroups; ++g) {
+            const uint32_t base = gfirst[g];
+            const uint32_t end = base + gcount[g];
+            float lox = INFINITY, loy = INFINITY, hix = -INFINITY, hiy = -INFINITY;
+            for (uint32_t s = base; s < end; ++s) {
+                const uint32_t b = ids[s];
+                lox = fminf(lox, pos[2 * b]); hix = fmaxf(hix, pos[2 * b]);
+                loy = fminf(loy, pos[2 * b + 1]); hiy = fmaxf(hiy, pos[2 * b + 1]);
+            }
+            size_t nn_ = 0, nr = 0;
+            int64_t sp = 0;
+            if (n > 1) stack[sp++] = 0;
+            while (sp > 0) {
+                ORC_GROW((size_t)sp + 2);
+                ORC_GROW(nn_ + 1);
+                ORC_GROW(nr + 1);
+                const uint32_t v = stack[--sp];
+                if (v >= nm1) { rfirst[nr] = v - nm1; rcount[nr++] = 1; continue; }
+                const float* bx = &aabb[4 * (size_t)v];
+                const float dx = fmaxf(0.0f, fmaxf(bx[0] - hix, lox - bx[2]));
+                const float dy = fmaxf(0.0f, fmaxf(bx[1] - hiy, loy - bx[3]));
+                const float d2 = dx * dx + dy * dy;
+                const float Ls = fmaxf(bx[2] - bx[0], bx[3] - bx[1]);
+                if (Ls * Ls < th2 * d2) {
+                    nodes[nn_++] = v;
+                } else if (last[v] - first[v] + 1 <= L) {
+                    rfirst[nr] = first[v];
+                    rcount[nr++] = last[v] - first[v] + 1;
+                } else {
+                    stack[sp++] = right[v];
+                    stack[sp++] = left[v];
+                }
+            }
+            for (uint32_t s = base; s < end; ++s) {
+                const uint32_t b = ids[s];
+                const float x = pos[2 * b], y = pos[2 * b + 1], m1 = mass[b];
+                float ax = 0.0f, ay = 0.0f;
+                for (size_t j = 0; j < nn_; ++j) {
+                    const uint32_t v = nodes[j];
+                    const float m2 = mass_node[v];
+                    const float rx = com[2 * (size_t)v] - x, ry = com[2 * (size_t)v + 1] - y;
+                    const float e2 = plummer ? eps2 : ecoef * fmaxf(m1, m2);
+                    const float r2 = rx * rx + ry * ry + e2;
+                    const float inv = 1.0f / sqrtf(r2);
+                    const float inv2 = inv * inv, inv3 = inv * inv2;
+                    if (p->multipole >= 2) {
+                        const float sxx = quad[3 * (size_t)v], sxy = quad[3 * (size_t)v + 1],
+                                    syy = quad[3 * (size_t)v + 2];
+                        const float tr = sxx + syy;
+                        const float qxx = 3.0f * sxx - tr, qxy = 3.0f * sxy, qyy = 3.0f * syy - tr;
+                        const float qrx = qxx * rx + qxy * ry, qry = qxy * rx + qyy * ry;
+                        const float rqr = rx * qrx + ry * qry;
+                        const float inv5 = inv3 * inv2;
+                        const float f = 2.5f * rqr * (inv5 * inv2) + m2 * inv3;
+                        ax += f * rx - qrx * inv5;
+                        ay += f * ry - qry * inv5;
+                    } else {
+                        const float f = m2 * inv3;
+                        ax += f * rx;
+                        ay += f * ry;
+                    }
+                }
+                for (size_t j = 0; j < nr; ++j) {
+                    for (uint32_t t = rfirst[j]; t < rfirst[j] + rcount[j]; ++t) {
+                        if (t == s) continue;
+                        const uint32_t bj = ids[t];
+                        const float rx = pos[2 * bj] - x, ry = pos[2 * bj + 1] - y;
+                        const float m2 = mass[bj];
+                        const float e2 = plummer ? eps2 : ecoef * fmaxf(m1, m2);
+                        const float inv = 1.0f / sqrtf(rx * rx + ry * ry + e2);
+                        const float f = m2 * (inv * inv * inv);
+                        ax += f * rx;
+                        ay += f * ry;
+                    }
+                }
+                acc[2 * b] = p->grav_constant * ax;
+                acc[2 * b + 1] = p->grav_constant * ay;
+            }
+        }
+#undef ORC_GROW
+        free(stack);
+        free(nodes);
+        free(rfirst);
+        free(rcount);
+    }
+    free(gfirst);
+    free(gcount);
+    free(first);
+    free(last);
+}
+
+/* ------------------------------------------------------------------------ */
 /* FP64 direct sum (accuracy oracle; no reference counterpart)               */
 /* ------------------------------------------------------------------------ */
 
@@ -470,6 +651,7 @@ struct orc_state {
     uint64_t* codes;
     uint32_t *ids, *left, *right, *parent;
     float *com, *mass_node, *aabb, *length;
+    float* quad; /* group walk: second moments */
 };
 
 orc_state* orc_create(const orc_params* p, uint32_t n, const float* mass, const float* pos,
@@ -492,6 +674,7 @@ orc_state* orc_create(const orc_params* p, uint32_t n, const float* mass, const 
     s->mass_node = (float*)calloc(nn, sizeof(float));
     s->aabb = (float*)calloc(4 * nn, sizeof(float));
     s->length = (float*)calloc(nn, sizeof(float));
+    s->quad = (float*)calloc(3 * nn, sizeof(float));
     if (n) {
         memcpy(s->mass, mass, sizeof(float) * n);
         memcpy(s->pos, pos, sizeof(float) * 2 * n);
@@ -504,7 +687,7 @@ void orc_destroy(orc_state* s) {
     if (!s) return;
     free(s->mass); free(s->pos); free(s->vel); free(s->acc);
     free(s->codes); free(s->ids); free(s->left); free(s->right); free(s->parent);
-    free(s->com); free(s->mass_node); free(s->aabb); free(s->length);
+    free(s->com); free(s->mass_node); free(s->aabb); free(s->length); free(s->quad);
     free(s);
 }
 
@@ -521,8 +704,14 @@ static void build_tree(orc_state* s) {
 
 static void forces(orc_state* s) {
     build_tree(s);
-    walk_impl(&s->p, s->n, s->ids, s->mass, s->pos, s->com, s->mass_node, s->length, s->left,
-              s->right, s->acc, NULL, NULL);
+    if (s->p.walk_mode == 1) {
+        orc_quadrupoles(s->n, s->left, s->right, s->com, s->mass_node, s->quad);
+        orc_walk_group(&s->p, s->n, s->ids, s->mass, s->pos, s->com, s->mass_node, s->aabb,
+                       s->quad, s->left, s->right, s->acc);
+    } else {
+        walk_impl(&s->p, s->n, s->ids, s->mass, s->pos, s->com, s->mass_node, s->length, s->left,
+                  s->right, s->acc, NULL, NULL);
+    }
     s->acc_valid = 1;
 }
 

@@ -54,6 +54,9 @@ typedef struct orc_params {
     int integrator;           /* ORC_INT_* */
     int leaf_size;            /* 1 = reference walk; >1 = direct sum over subtrees of <= leaf_size bodies */
     int threads;              /* OpenMP threads for the parallel baseline (0 = all) */
+    int walk_mode;            /* 0 = reference per-body walk, 1 = group walk (extension) */
+    int multipole;            /* group walk: 1 monopole, 2 monopole + quadrupole */
+    int bodies_per_lane;      /* group walk: group = 32 * bodies_per_lane consecutive sorted slots */
 } orc_params;
 
 /* Domain used by the Morton encode: scale/offset for 32-bit keys, or the
@@ -87,6 +90,20 @@ void orc_fill(uint32_t n, uint32_t offset, const uint32_t* ids, const float* mas
 void orc_walk(const orc_params* p, uint32_t n, const uint32_t* ids, const float* mass,
               const float* pos, const float* com, const float* mass_node, const float* length,
               const uint32_t* left, const uint32_t* right, float* acc);
+
+/* Extension: second moments about each node's COM, quad[3*(2n-1)] = {Sxx, Sxy, Syy}
+ * (leaves 0), combined left child first: S = sum_c S_c + m_c d_c d_c^T. */
+void orc_quadrupoles(uint32_t n, const uint32_t* left, const uint32_t* right, const float* com,
+                     const float* mass_node, float* quad);
+
+/* Extension: group walk.  Groups are the maximal subtrees of at most
+ * 32*bodies_per_lane bodies (contiguous sorted slots); a group opens a node unless L^2 < theta^2 d^2 (L = longest side of the node's
+ * box, d = distance between the group's box and the node's box); accepted
+ * nodes act through monopole (+ quadrupole), leaves and opened nodes of
+ * <= leaf_size bodies body by body.  acc[2*body]. */
+void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const float* mass,
+                    const float* pos, const float* com, const float* mass_node, const float* aabb,
+                    const float* quad, const uint32_t* left, const uint32_t* right, float* acc);
 
 /* Node visit / interaction counters of the same walk (for rooflines). */
 void orc_walk_counts(const orc_params* p, uint32_t n, const uint32_t* ids, const float* mass,

@@ -33,7 +33,13 @@ class OrcParams(ctypes.Structure):
         ("integrator", ctypes.c_int),
         ("leaf_size", ctypes.c_int),
         ("threads", ctypes.c_int),
+        ("walk_mode", ctypes.c_int),
+        ("multipole", ctypes.c_int),
+        ("bodies_per_lane", ctypes.c_int),
     ]
+
+
+WALK = {"exact": 0, "group": 1}
 
 
 class OrcDomain(ctypes.Structure):
@@ -90,9 +96,11 @@ def _p(a):
 
 def params(G=1.0, dt=0.1 / 60.0, eps_mult=1.0, theta=0.6, softening="reference",
            plummer_eps=1e-3, morton_bits=32, morton_domain="fixed2000",
-           integrator="symplectic-euler", leaf_size=1, threads=0) -> OrcParams:
+           integrator="symplectic-euler", leaf_size=1, threads=0, walk="exact", multipole=2,
+           bodies_per_lane=2) -> OrcParams:
     return OrcParams(G, dt, eps_mult, theta, SOFT[softening], plummer_eps, morton_bits,
-                     DOMAIN[morton_domain], INTEGRATOR[integrator], leaf_size, threads)
+                     DOMAIN[morton_domain], INTEGRATOR[integrator], leaf_size, threads,
+                     WALK[walk], multipole, bodies_per_lane)
 
 
 def params_from_config(cfg, threads: int = 0) -> OrcParams:
@@ -100,7 +108,9 @@ def params_from_config(cfg, threads: int = 0) -> OrcParams:
     return params(G=cfg.gravConstant, dt=cfg.deltaTime, eps_mult=cfg.epsilonMultiplier,
                   theta=cfg.bhTheta, softening=cfg.softening, plummer_eps=cfg.plummerEps,
                   morton_bits=cfg.mortonBits, morton_domain=cfg.mortonDomain,
-                  integrator=cfg.integrator, leaf_size=cfg.leafSize, threads=threads)
+                  integrator=cfg.integrator, leaf_size=cfg.leafSize, threads=threads,
+                  walk=getattr(cfg, "walk", "exact"), multipole=getattr(cfg, "multipole", 2),
+                  bodies_per_lane=getattr(cfg, "bodiesPerLane", 2) or 2)
 
 
 def f32(a, shape=None):

@@ -173,6 +173,90 @@ def test_profile_and_kernel_count(bh):
     sim.close()
 
 
+GROUP = dict(walk="group", softening="plummer", plummerEps=1e-3, bhTheta=0.5,
+             mortonDomain="bbox", leafSize=8)
+
+
+@pytest.mark.parametrize("bpl", [1, 2, 4])
+@pytest.mark.parametrize("mp", [1, 2])
+def test_group_walk_matches_oracle(bh, orc, bpl, mp):
+    # Same interaction lists as the oracle (the criterion only reads exact
+    # boxes); values differ by rsqrt/FMA rounding and the FP64 top levels.
+    sim = make_sim(bh, 30000, "colliding-disks", seed=3, **dict(GROUP, multipole=mp,
+                                                                bodiesPerLane=bpl))
+    acc, acc_ref = compare_tree(orc, sim)
+    err = acc_errors(acc, acc_ref)
+    assert np.median(err) <= 1e-5
+    assert err.max() <= 1e-3
+    sim.close()
+
+
+@pytest.mark.parametrize("n", [2, 3, 31, 33, 64, 65, 129])
+def test_group_walk_small_n(bh, orc, n):
+    sim = make_sim(bh, n, "uniform-disk-kepler", seed=n, **GROUP)
+    acc, acc_ref = compare_tree(orc, sim)
+    err = acc_errors(acc, acc_ref)
+    assert err.max() <= 1e-4
+    sim.close()
+
+
+def test_group_walk_reference_softening(bh, orc):
+    sim = make_sim(bh, 20000, "default", seed=6, walk="group", bhTheta=0.5, leafSize=4)
+    acc, acc_ref = compare_tree(orc, sim)
+    err = acc_errors(acc, acc_ref)
+    assert np.median(err) <= 1e-5
+    sim.close()
+
+
+def test_group_walk_64bit_duplicates(bh, orc):
+    sim = make_sim(bh, 100000, "gaussian-mixture", seed=9,
+                   **dict(GROUP, mortonBits=64, plummerEps=1e-4))
+    acc, acc_ref = compare_tree(orc, sim)
+    err = acc_errors(acc, acc_ref)
+    assert np.median(err) <= 1e-5
+    assert (err > 1e-4).mean() <= 0.001
+    sim.close()
+
+
+def test_group_walk_accuracy_800k_vs_fp64(bh, orc):
+    # The benchmark workload: median relative force error <= 1e-3 at theta 0.5.
+    sim = make_sim(bh, 800_000, "colliding-disks", seed=1, **GROUP)
+    mass, pos, vel = sim.download()
+    acc = sim.computeAccelerations()
+    sample = np.random.default_rng(0).choice(800_000, 300, replace=False)
+    ref = orc.direct_sum_fp64(orc.params_from_config(sim.config), mass, pos, sample)
+    err = np.linalg.norm(acc[sample] - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    assert np.median(err) <= 1e-3
+    sim.close()
+
+
+def test_group_walk_kdk_steps_match_oracle(bh, orc):
+    sim = make_sim(bh, 20000, "colliding-disks", seed=8,
+                   **dict(GROUP, integrator="leapfrog-kdk", deltaTime=5e-5))
+    mass, pos, vel = sim.download()
+    st = orc.State(oracle_params(orc, sim), mass, pos, vel)
+    sim.step(4)
+    sim.sync()
+    st.step(4)
+    _, p_gpu, v_gpu = sim.download()
+    p_ref, v_ref = st.state()
+    assert np.abs(v_gpu - v_ref).max() <= 1e-4 * np.abs(v_ref).max()
+    assert np.abs(p_gpu - p_ref).max() <= 1e-5 * (np.abs(p_ref).max() + 1)
+    sim.close()
+
+
+def test_walk_stats_counts(bh):
+    sim = make_sim(bh, 50000, "colliding-disks", seed=2, **GROUP)
+    visits, multi, body = sim.walk_stats()
+    assert visits > 0 and multi > 0 and body > 0
+    sim2 = make_sim(bh, 50000, "colliding-disks", seed=2, softening="plummer", bhTheta=0.5,
+                    mortonDomain="bbox")
+    v2, m2, b2 = sim2.walk_stats()
+    assert v2 > 0 and m2 > 0 and b2 > 0
+    sim.close()
+    sim2.close()
+
+
 def test_unknown_scenario_raises(bh):
     sim = bh.Simulation()
     with pytest.raises(bh.BhError, match="Unknown scenario: nope"):

@@ -168,6 +168,53 @@ def test_reference_monopole_walk_accuracy_vs_fp64(orc):
     assert med[0] < 5e-2 and med[1] < med[0] and med[2] < med[1] and med[2] < 2e-3
 
 
+def test_quadrupole_of_two_points(orc):
+    # Two unit masses at (-1, 0) and (1, 0): COM 0, Sxx = 2, Sxy = Syy = 0.
+    keys = np.array([1, 2], np.uint64)
+    left, right, parent = orc.build(keys, 32)
+    mass = np.ones(2, np.float32)
+    pos = np.array([[-1, 0], [1, 0]], np.float32)
+    com, mnode, aabb, length = orc.fill(np.arange(2, dtype=np.uint32), mass, pos, left, right, parent)
+    quad = np.zeros((3, 3), np.float32)
+    orc.load().orc_quadrupoles(2, orc._p(left), orc._p(right), orc._p(com), orc._p(mnode),
+                               orc._p(quad))
+    assert quad[0].tolist() == [2.0, 0.0, 0.0]
+
+
+def test_quadrupole_far_field_matches_direct_sum(orc):
+    # A tight cluster seen from far away: the quadrupole term cuts the
+    # monopole error by at least 10x.
+    rng = np.random.default_rng(8)
+    n = 64
+    cluster = (rng.normal(size=(n, 2)) * [0.3, 0.1]).astype(np.float32)
+    probe = np.array([[3.0, 1.0]], np.float32)
+    pos = np.concatenate([cluster, probe])
+    mass = np.concatenate([rng.uniform(0.5, 1.5, n), [1e-6]]).astype(np.float32)
+    ref = orc.direct_sum_fp64(orc.params(softening="plummer", plummer_eps=1e-4), mass, pos, [n])
+    errs = {}
+    for mp in (1, 2):
+        # theta large enough that the probe's group accepts the cluster's root
+        p = orc.params(theta=1.5, softening="plummer", plummer_eps=1e-4, morton_domain="bbox",
+                       walk="group", multipole=mp, bodies_per_lane=1)
+        acc = orc.State(p, mass, pos, np.zeros_like(pos)).accelerations()
+        errs[mp] = np.linalg.norm(acc[n] - ref[0]) / np.linalg.norm(ref[0])
+    assert errs[2] < errs[1] / 10
+
+
+def test_group_walk_theta05_meets_1e3(orc, bh):
+    # The engine's group walk (quadrupoles, leaf buckets of 8) at theta = 0.5:
+    # median relative force error <= 1e-3 against the FP64 direct sum.
+    for scenario in ("colliding-disks", "uniform-disk-kepler", "gaussian-mixture"):
+        mass, pos, vel, _ = bh.generate_scenario(scenario, 30000, seed=2)
+        p = orc.params(theta=0.5, softening="plummer", plummer_eps=1e-3, morton_domain="bbox",
+                       walk="group", multipole=2, leaf_size=8, bodies_per_lane=2)
+        acc = orc.State(p, mass, pos, vel).accelerations()
+        sample = np.arange(0, 30000, 97)
+        ref = orc.direct_sum_fp64(p, mass, pos, sample)
+        err = np.linalg.norm(acc[sample] - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        assert np.median(err) < 1e-3, (scenario, np.median(err))
+
+
 def test_results_do_not_depend_on_thread_count(orc):
     rng = np.random.default_rng(5)
     n = 3000

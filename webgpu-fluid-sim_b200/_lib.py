@@ -46,8 +46,15 @@ class bh_config(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("use_graphs", ctypes.c_int32),
         ("fp64_levels", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("walk_mode", ctypes.c_int32),
+        ("multipole_order", ctypes.c_int32),
+        ("bodies_per_lane", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
     ]
+
+
+BH_WALK_EXACT = 0
+BH_WALK_GROUP = 1
 
 
 class bh_buffers(ctypes.Structure):
@@ -94,6 +101,7 @@ SIGNATURES = {
                                       ctypes.POINTER(ctypes.c_uint32)]),
     "bh_kernels_per_step": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint32)]),
     "bh_walk_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64),
+                                     ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_uint64)]),
     "bh_build_hierarchy_static": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _P, ctypes.c_uint32,
                                                  _P, _P, _P, _P, ctypes.c_int32, _P]),

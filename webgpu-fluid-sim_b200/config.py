@@ -30,6 +30,9 @@ class Config:
     walkBlock: int = 0
     useGraphs: bool = True
     fp64Levels: bool = True
+    walk: str = "exact"                 # "exact" (reference per-body walk) | "group"
+    multipole: int = 2                  # group walk: 1 monopole, 2 + quadrupole
+    bodiesPerLane: int = 2              # group walk: group = 32 x bodiesPerLane bodies
 
     def to_c(self, device: int = 0) -> _lib.bh_config:
         c = _lib.bh_config()
@@ -51,6 +54,9 @@ class Config:
         c.device = device
         c.use_graphs = 1 if self.useGraphs else 0
         c.fp64_levels = 1 if self.fp64Levels else 0
+        c.walk_mode = {"exact": _lib.BH_WALK_EXACT, "group": _lib.BH_WALK_GROUP}[self.walk]
+        c.multipole_order = self.multipole
+        c.bodies_per_lane = self.bodiesPerLane
         return c
 
 
@@ -61,21 +67,25 @@ def getDefaultConfig() -> Config:
                   deltaTime=0.1 * 1.0 / (60.0 * substeps), epsilonMultiplier=1.0)
 
 
-# The seeded benchmark workloads (Plummer softening, leapfrog), by name.
+# The seeded benchmark workloads (Plummer softening, leapfrog, group walk with
+# quadrupoles, leaf buckets of 8), by name.
 WORKLOADS = {
     # N=16,384 uniform disk, theta 0.7, eps 1e-3, dt 1e-4, 32-bit keys over the bbox
     "uniform-disk-16k": dict(n=16384, scenario="uniform-disk-kepler", steps=100,
                              config=Config(bhTheta=0.7, deltaTime=1e-4, softening="plummer",
                                            plummerEps=1e-3, mortonDomain="bbox",
-                                           integrator="leapfrog-kdk")),
+                                           integrator="leapfrog-kdk", walk="group",
+                                           leafSize=8)),
     # N=800,000 two colliding exponential disks, theta 0.5, eps 1e-3, dt 5e-5
     "colliding-disks-800k": dict(n=800_000, scenario="colliding-disks", steps=1000,
                                  config=Config(bhTheta=0.5, deltaTime=5e-5, softening="plummer",
                                                plummerEps=1e-3, mortonDomain="bbox",
-                                               integrator="leapfrog-kdk")),
+                                               integrator="leapfrog-kdk", walk="group",
+                                               leafSize=8)),
     # N=16,777,216 Gaussian mixture, 64-bit keys, theta 0.5, eps 1e-4, dt 1e-5
     "gaussian-mixture-16m": dict(n=16_777_216, scenario="gaussian-mixture", steps=50,
                                  config=Config(bhTheta=0.5, deltaTime=1e-5, softening="plummer",
                                                plummerEps=1e-4, mortonBits=64,
-                                               integrator="leapfrog-kdk")),
+                                               integrator="leapfrog-kdk", walk="group",
+                                               leafSize=8)),
 }

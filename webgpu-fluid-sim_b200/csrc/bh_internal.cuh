@@ -29,6 +29,22 @@ constexpr uint32_t kErrLookbackSpin = 1u << 0;  // decoupled look-back gave up w
 constexpr uint32_t kErrStackOverflow = 1u << 1; // walk stack would have overflowed (children dropped)
 constexpr uint32_t kErrTreeSpin = 1u << 2;
 
+// Packed internal-node record of the group walk (64 B, one per internal node):
+// the criterion reads `box`, an accepted node contributes `mom` + `quad`, an
+// opened node continues through `link`.
+struct __align__(16) GNode {
+    float4 box;   // {min.x, min.y, max.x, max.y}
+    float4 mom;   // {com.x, com.y, mass, length}
+    float4 quad;  // raw second moments about the COM {Sxx, Sxy, Syy, 0}
+    uint4 link;   // {left, right, first slot, body count}
+};
+
+// Group-walk stack and list capacities (per warp).
+constexpr int kGroupStack = 1024;
+constexpr int kGroupDfsAt = kGroupStack - 128;  // switch to one node per step above this depth
+constexpr int kGroupList = 64;
+constexpr uint32_t kErrGroupStack = 1u << 3;    // group-walk stack overflow (never expected)
+
 // Walk modes.
 enum WalkMode : int {
     kWalkForces = 0,       // acc[b] = a
@@ -47,7 +63,12 @@ struct WalkParams {
     int leaf_size;    // bucket size (1 = reference walk)
     int mode;         // WalkMode
     int count;        // 1 = instrumented launch: accumulate visit/interaction counters
-    unsigned long long* counters;  // {node visits, interactions} when count == 1
+    unsigned long long* counters;  // exact walk: {node visits, interactions};
+                                   // group walk: {node visits, node interactions, body interactions}
+    // group walk
+    int multipole;    // 1 or 2
+    int bpl;          // bodies per lane
+    unsigned int* group_ctr;  // dynamic group counter (zeroed per step)
 };
 
 // Per-step scratch that must start at zero.  One memset clears it.
@@ -55,7 +76,8 @@ struct StepScratch {
     uint32_t hist[8][kRadix];  // digit histograms per pass
     uint32_t tile_ctr[8];      // dynamic tile counters per pass
     uint32_t bbox[4];          // ordered-int max of {-minx, -miny, maxx, maxy} (see morton.cu)
-    unsigned long long walk_counts[2];  // instrumented walk: {node visits, interactions}
+    unsigned long long walk_counts[4];  // instrumented walk counters
+    unsigned int group_ctr[4];          // group walk: [0] work counter, [1] number of groups
 };
 
 struct DeviceBuffers {
@@ -81,6 +103,9 @@ struct DeviceBuffers {
     uint2* range = nullptr;      // n-1 {first slot, last slot}
     double2* big = nullptr;      // 2(n-1) FP64 {mass, mass*x}, {mass*y, 0} for big nodes
     uint32_t* bound = nullptr;   // n-1 exchange slots, kSentinel between steps
+    GNode* gnode = nullptr;      // n-1 packed records (group walk only; else null)
+    uint2* groups = nullptr;     // n {first slot, count}: maximal subtrees of <= G bodies (group walk)
+    uint32_t group_max = 0;      // G = 32 x bodies per lane (0: no groups)
     // scratch
     StepScratch* scratch = nullptr;
     uint32_t* status = nullptr;  // look-back status: passes * tiles * 256
@@ -104,5 +129,7 @@ void launch_build_fill(const DeviceBuffers& b, int fp64_levels, cudaStream_t s);
 void init_bound(const DeviceBuffers& b, cudaStream_t s);
 // walk.cu
 void launch_walk(const DeviceBuffers& b, const WalkParams& p, int block, cudaStream_t s);
+// walk_group.cu
+void launch_walk_group(const DeviceBuffers& b, const WalkParams& p, int block, cudaStream_t s);
 
 }  // namespace bh

@@ -93,6 +93,9 @@ extern "C" int bh_default_config(bh_config* out) {
     out->device = 0;
     out->use_graphs = 1;
     out->fp64_levels = 1;
+    out->walk_mode = BH_WALK_EXACT;
+    out->multipole_order = 2;
+    out->bodies_per_lane = 2;
     return BH_OK;
 }
 
@@ -108,6 +111,13 @@ static int validate_config(bh_sim* s, const bh_config& c) {
     if (c.substeps < 1) return fail(s, BH_ERR_INVALID_ARGUMENT, "substeps must be >= 1");
     if (c.leaf_size < 1 || c.leaf_size > 64)
         return fail(s, BH_ERR_INVALID_ARGUMENT, "leaf_size must be in [1, 64]");
+    if (c.walk_mode != BH_WALK_EXACT && c.walk_mode != BH_WALK_GROUP)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "unknown walk_mode");
+    if (c.walk_mode == BH_WALK_GROUP && c.multipole_order != 1 && c.multipole_order != 2)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "multipole_order must be 1 or 2");
+    if (c.walk_mode == BH_WALK_GROUP && c.bodies_per_lane != 0 && c.bodies_per_lane != 1 &&
+        c.bodies_per_lane != 2 && c.bodies_per_lane != 4)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "bodies_per_lane must be 1, 2 or 4");
     if (!(c.delta_time == c.delta_time) || !(c.bh_theta >= 0.0f))
         return fail(s, BH_ERR_INVALID_ARGUMENT, "delta_time must be a number and bh_theta >= 0");
     return BH_OK;
@@ -155,6 +165,9 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     size_t o_node4 = c.take<float4>(nn), o_child = c.take<uint2>(ni), o_parent = c.take<uint32_t>(nn);
     size_t o_aabb = c.take<float4>(ni), o_range = c.take<uint2>(ni), o_big = c.take<double2>(2 * ni);
     size_t o_bound = c.take<uint32_t>(ni);
+    const bool group = s->cfg.walk_mode == BH_WALK_GROUP;
+    size_t o_gnode = group ? c.take<bh::GNode>(ni) : 0;
+    size_t o_groups = group ? c.take<uint2>(nb) : 0;
     size_t o_scr = c.take<bh::StepScratch>(1);
     size_t o_status = c.take<uint32_t>((size_t)kb * (tiles ? tiles : 1) * bh::kRadix);
     size_t o_err = c.take<uint32_t>(1);
@@ -187,6 +200,9 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     b.range = (uint2*)(a + o_range);
     b.big = (double2*)(a + o_big);
     b.bound = (uint32_t*)(a + o_bound);
+    b.gnode = group ? (bh::GNode*)(a + o_gnode) : nullptr;
+    b.groups = group ? (uint2*)(a + o_groups) : nullptr;
+    b.group_max = group ? 32u * (uint32_t)(s->cfg.bodies_per_lane > 0 ? s->cfg.bodies_per_lane : 2) : 0u;
     b.scratch = (bh::StepScratch*)(a + o_scr);
     b.status = (uint32_t*)(a + o_status);
     b.tiles = tiles;
@@ -215,7 +231,15 @@ static bh::WalkParams walk_params(const bh_sim* s, int mode) {
     p.mode = mode;
     p.count = 0;
     p.counters = nullptr;
+    p.multipole = c.multipole_order;
+    p.bpl = c.bodies_per_lane > 0 ? c.bodies_per_lane : 2;
+    p.group_ctr = s->b.scratch ? s->b.scratch->group_ctr : nullptr;
     return p;
+}
+
+static void launch_walk_any(bh_sim* s, const bh::WalkParams& p) {
+    if (s->cfg.walk_mode == BH_WALK_GROUP) bh::launch_walk_group(s->b, p, s->cfg.walk_block, s->stream);
+    else bh::launch_walk(s->b, p, s->cfg.walk_block, s->stream);
 }
 
 static bool needs_bbox(const bh_sim* s) {
@@ -246,8 +270,7 @@ static void enqueue_step(bh_sim* s, Mark mark) {
     mark(0);
     if (kdk) bh::launch_kick_drift(s->b, s->cfg.delta_time, s->stream);
     enqueue_tree(s, mark);
-    bh::launch_walk(s->b, walk_params(s, kdk ? bh::kWalkKdkClose : bh::kWalkEulerKickDrift),
-                    s->cfg.walk_block, s->stream);
+    launch_walk_any(s, walk_params(s, kdk ? bh::kWalkKdkClose : bh::kWalkEulerKickDrift));
     mark(5);
 }
 
@@ -255,7 +278,7 @@ template <class Mark>
 static void enqueue_forces(bh_sim* s, Mark mark) {
     mark(0);
     enqueue_tree(s, mark);
-    bh::launch_walk(s->b, walk_params(s, bh::kWalkForces), s->cfg.walk_block, s->stream);
+    launch_walk_any(s, walk_params(s, bh::kWalkForces));
     mark(5);
 }
 
@@ -533,15 +556,16 @@ extern "C" int bh_compute_accelerations(bh_sim* s, float* acc_host) {
     return check_device_errors(s);
 }
 
-extern "C" int bh_walk_stats(bh_sim* s, uint64_t* node_visits, uint64_t* interactions) {
+extern "C" int bh_walk_stats(bh_sim* s, uint64_t* node_visits, uint64_t* multipole_interactions,
+                             uint64_t* body_interactions) {
     BH_HANDLE(s);
-    unsigned long long h[2] = {0, 0};
+    unsigned long long h[3] = {0, 0, 0};
     if (s->b.n > 0) {
         enqueue_tree(s, [](int) {});
         bh::WalkParams p = walk_params(s, bh::kWalkForces);
         p.count = 1;
         p.counters = s->b.scratch->walk_counts;
-        bh::launch_walk(s->b, p, s->cfg.walk_block, s->stream);
+        launch_walk_any(s, p);
         BH_CUDA(s, cudaGetLastError());
         BH_CUDA(s, cudaMemcpyAsync(h, s->b.scratch->walk_counts, sizeof(h), cudaMemcpyDeviceToHost,
                                    s->stream));
@@ -549,7 +573,8 @@ extern "C" int bh_walk_stats(bh_sim* s, uint64_t* node_visits, uint64_t* interac
         s->acc_valid = true;
     }
     if (node_visits) *node_visits = h[0];
-    if (interactions) *interactions = h[1];
+    if (multipole_interactions) *multipole_interactions = h[1];
+    if (body_interactions) *body_interactions = h[2];
     return check_device_errors(s);
 }
 

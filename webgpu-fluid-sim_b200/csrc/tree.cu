@@ -14,11 +14,13 @@ void launch_build_fill(const DeviceBuffers& b, int fp64_levels, cudaStream_t s) 
     if (b.key_bytes == 8)
         build_fill_kernel<uint64_t><<<blocks, 256, 0, s>>>(
             (const uint64_t*)b.codes, b.ids, b.mass, b.pos, b.node4, b.children, b.parent, b.aabb,
-            b.range, b.big, b.bound, b.n, fp64_levels);
+            b.range, b.big, b.bound, b.n, fp64_levels, b.gnode, b.groups,
+            b.groups ? &b.scratch->group_ctr[1] : nullptr, b.group_max);
     else
         build_fill_kernel<uint32_t><<<blocks, 256, 0, s>>>(
             (const uint32_t*)b.codes, b.ids, b.mass, b.pos, b.node4, b.children, b.parent, b.aabb,
-            b.range, b.big, b.bound, b.n, fp64_levels);
+            b.range, b.big, b.bound, b.n, fp64_levels, b.gnode, b.groups,
+            b.groups ? &b.scratch->group_ctr[1] : nullptr, b.group_max);
 }
 
 }  // namespace bh

@@ -51,7 +51,9 @@ build_fill_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ ids,
                   float4* __restrict__ node4, uint2* __restrict__ children,
                   uint32_t* __restrict__ parent, float4* __restrict__ aabb,
                   uint2* __restrict__ range, double2* __restrict__ big,
-                  uint32_t* __restrict__ bound, uint32_t n, int fp64) {
+                  uint32_t* __restrict__ bound, uint32_t n, int fp64,
+                  GNode* __restrict__ gnode, uint2* __restrict__ groups,
+                  unsigned int* __restrict__ group_count, uint32_t gmax) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t nm1 = n - 1;
@@ -61,12 +63,17 @@ build_fill_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ ids,
     node4[nm1 + i] = make_float4(p.x, p.y, m, 0.0f);  // leaf (lbvh.wgsl:179-187)
     if (n == 1) {
         parent[0] = kSentinel;
+        if (groups) {
+            groups[0] = make_uint2(0u, 1u);
+            *group_count = 1u;
+        }
         return;
     }
     // Running record of the node this thread currently owns.
     float cm = m, cx = p.x, cy = p.y;
     float lox = p.x, loy = p.y, hix = p.x, hiy = p.y;
     double dm = 0.0, dmx = 0.0, dmy = 0.0;  // valid when the node has >= kFp64MinBodies bodies
+    float sxx = 0.0f, sxy = 0.0f, syy = 0.0f;  // second moments about the COM (group walk)
     uint32_t l = i, r = i;
     while (true) {
         const int dl = (l == 0) ? -1 : delta_at(keys, l - 1, l);
@@ -136,6 +143,43 @@ build_fill_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ ids,
             }
         }
         const float len = fmaxf(__fsub_rn(hix, lox), __fsub_rn(hiy, loy));
+        if (gnode) {
+            // Second moments about the parent COM, left child first:
+            // S = sum_c S_c + m_c d_c d_c^T, d_c = c_c - c_parent (leaves: S_c = 0).
+            float4 sq = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (sib < nm1) sq = __ldcg(&gnode[sib].quad);
+            float ml, mr, lxx, lxy, lyy, rxx, rxy, ryy, dlx, dly, drx, dry;
+            if (is_left) {
+                ml = cm; lxx = sxx; lxy = sxy; lyy = syy; dlx = __fsub_rn(cx, ncx); dly = __fsub_rn(cy, ncy);
+                mr = s4.z; rxx = sq.x; rxy = sq.y; ryy = sq.z; drx = __fsub_rn(s4.x, ncx); dry = __fsub_rn(s4.y, ncy);
+            } else {
+                ml = s4.z; lxx = sq.x; lxy = sq.y; lyy = sq.z; dlx = __fsub_rn(s4.x, ncx); dly = __fsub_rn(s4.y, ncy);
+                mr = cm; rxx = sxx; rxy = sxy; ryy = syy; drx = __fsub_rn(cx, ncx); dry = __fsub_rn(cy, ncy);
+            }
+            sxx = __fadd_rn(__fadd_rn(lxx, __fmul_rn(ml, __fmul_rn(dlx, dlx))),
+                            __fadd_rn(rxx, __fmul_rn(mr, __fmul_rn(drx, drx))));
+            sxy = __fadd_rn(__fadd_rn(lxy, __fmul_rn(ml, __fmul_rn(dlx, dly))),
+                            __fadd_rn(rxy, __fmul_rn(mr, __fmul_rn(drx, dry))));
+            syy = __fadd_rn(__fadd_rn(lyy, __fmul_rn(ml, __fmul_rn(dly, dly))),
+                            __fadd_rn(ryy, __fmul_rn(mr, __fmul_rn(dry, dry))));
+            GNode g;
+            g.box = make_float4(lox, loy, hix, hiy);
+            g.mom = make_float4(ncx, ncy, tm, len);
+            g.quad = make_float4(sxx, sxy, syy, 0.0f);
+            g.link = make_uint4(li, ri, pl, cnt);
+            gnode[pidx] = g;
+        }
+        if (groups) {
+            // Walk groups: maximal subtrees of <= gmax bodies.  A child is one
+            // when its parent is too big; the whole tree is one when n <= gmax.
+            if (cnt > gmax) {
+                const uint32_t lcnt = gamma - pl + 1, rcnt = pr - gamma;
+                if (lcnt <= gmax) groups[atomicAdd(group_count, 1u)] = make_uint2(pl, lcnt);
+                if (rcnt <= gmax) groups[atomicAdd(group_count, 1u)] = make_uint2(gamma + 1, rcnt);
+            } else if (pidx == 0) {
+                groups[atomicAdd(group_count, 1u)] = make_uint2(0u, n);
+            }
+        }
         node4[pidx] = make_float4(ncx, ncy, tm, len);
         aabb[pidx] = make_float4(lox, loy, hix, hiy);
         children[pidx] = make_uint2(li, ri);

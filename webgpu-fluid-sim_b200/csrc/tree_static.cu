@@ -114,11 +114,11 @@ extern "C" int bh_build_hierarchy_static(const void* sorted_codes, int32_t morto
     if (morton_bits == 64)
         build_fill_kernel<uint64_t><<<blocks, 256, 0, s>>>(
             static_cast<const uint64_t*>(sorted_codes), sorted_ids, mass, p2, n4, ch, node_parent,
-            bx, range, big, bound, n, fp64_levels);
+            bx, range, big, bound, n, fp64_levels, nullptr, nullptr, nullptr, 0u);
     else
         build_fill_kernel<uint32_t><<<blocks, 256, 0, s>>>(
             static_cast<const uint32_t*>(sorted_codes), sorted_ids, mass, p2, n4, ch, node_parent,
-            bx, range, big, bound, n, fp64_levels);
+            bx, range, big, bound, n, fp64_levels, nullptr, nullptr, nullptr, 0u);
     e = cudaGetLastError();
     if (e != cudaSuccess)
         return static_fail(BH_ERR_CUDA, std::string("build_fill_kernel launch: ") + cudaGetErrorString(e));

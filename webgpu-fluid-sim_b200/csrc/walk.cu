@@ -45,7 +45,7 @@ walk_kernel(const float4* __restrict__ node4, const uint2* __restrict__ children
     const float4 me = active ? __ldg(&node4[my_leaf]) : make_float4(0.f, 0.f, 0.f, 0.f);
     float ax = 0.0f, ay = 0.0f;
     const bool counting = MODE == kWalkForces && P.count;
-    uint32_t n_vis = 0, n_int = 0;  // instrumented launch only
+    uint32_t n_vis = 0, n_node = 0, n_body = 0;  // instrumented launch only
     uint2* stk = s_stack[w];
     if (lane == 0) stk[0] = make_uint2(0u, act);
     int sp = 1;
@@ -64,7 +64,8 @@ walk_kernel(const float4* __restrict__ node4, const uint2* __restrict__ children
         const bool far = leaf || (nd.w * inv < P.theta);
         if (counting) {
             n_vis += in;
-            n_int += in && far && node != my_leaf;
+            n_node += in && far && !leaf;
+            n_body += in && leaf && node != my_leaf;
         }
         if (in && far && node != my_leaf) {
             const float f = P.g * nd.z * (inv * inv * inv);
@@ -83,7 +84,7 @@ walk_kernel(const float4* __restrict__ node4, const uint2* __restrict__ children
                         const float q2 = qx * qx + qy * qy;
                         const float f2 = PLUMMER ? P.eps2 : P.eps_coef * fmaxf(me.z, bj.z);
                         const float iv = rsqrtf(q2 + f2);
-                        if (counting) n_int += mine && s != slot;
+                        if (counting) n_body += mine && s != slot;
                         if (mine && s != slot) {
                             const float f = P.g * bj.z * (iv * iv * iv);
                             ax = fmaf(f, qx, ax);
@@ -107,15 +108,17 @@ walk_kernel(const float4* __restrict__ node4, const uint2* __restrict__ children
         __syncwarp();
     }
     if (counting) {
-        unsigned long long v = n_vis, it = n_int;
+        unsigned long long v = n_vis, nd = n_node, bd = n_body;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-            it += __shfl_xor_sync(0xFFFFFFFFu, it, o);
+            nd += __shfl_xor_sync(0xFFFFFFFFu, nd, o);
+            bd += __shfl_xor_sync(0xFFFFFFFFu, bd, o);
         }
         if (lane == 0) {
             atomicAdd(&P.counters[0], v);
-            atomicAdd(&P.counters[1], it);
+            atomicAdd(&P.counters[1], nd);
+            atomicAdd(&P.counters[2], bd);
         }
     }
     if (!active) return;

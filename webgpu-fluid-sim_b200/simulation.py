@@ -203,12 +203,14 @@ class Simulation:
         self._check(self._lib.bh_profile_end(self._h, ms, ctypes.byref(cnt)))
         return {k: float(ms[i]) for i, k in enumerate(_lib.BH_STAGE_NAMES)}, int(cnt.value)
 
-    def walk_stats(self) -> tuple[int, int]:
-        """(node visits, interactions) summed over all bodies at the current positions."""
+    def walk_stats(self) -> tuple[int, int, int]:
+        """(node visits, multipole interactions, body interactions) at the current positions."""
         v = ctypes.c_uint64()
-        i = ctypes.c_uint64()
-        self._check(self._lib.bh_walk_stats(self._h, ctypes.byref(v), ctypes.byref(i)))
-        return int(v.value), int(i.value)
+        m = ctypes.c_uint64()
+        b = ctypes.c_uint64()
+        self._check(self._lib.bh_walk_stats(self._h, ctypes.byref(v), ctypes.byref(m),
+                                            ctypes.byref(b)))
+        return int(v.value), int(m.value), int(b.value)
 
     def kernels_per_step(self) -> int:
         k = ctypes.c_uint32()
