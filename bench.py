@@ -16,9 +16,11 @@ Own arm (default):
              in the step graph during the timed steps.
   cpu_baseline  the oracle (C restatement, OpenMP, all host threads) on a
              bounded sample of the same workload.
-Reference arm (--impl reference): the reference's algorithm on the host
-cores (the oracle port; the reference itself is WGSL and needs a WebGPU
-device, which this machine lacks).
+Reference arm (--impl reference): the reference's own pipeline logic on the
+host cores: its WGSL compute shaders mechanically translated to C++
+(oracle/_ref, built where the reference checkout exists), all host threads;
+if that build is absent, the oracle port.  The WGSL itself needs a WebGPU
+device, which this machine lacks.
 
 Multi-GPU (torchrun): every rank simulates its own independently seeded copy
 of the workload (weak scaling, no collective on the data path); the timed
@@ -137,7 +139,44 @@ def force_error_vs_fp64(acc, mass, pos, cfg, nsample=256, seed=0):
     return float(np.median(errs)), float(np.percentile(errs, 99)), int(idx.size)
 
 
+def reference_baseline(pkg, wl, seconds_budget=20.0):
+    """The reference's own shader logic (oracle/_ref: a mechanical C++
+    translation of lbvh.wgsl + barnes_hut.wgsl, independent stages on all host
+    threads) on the workload's bodies, theta and dt.  The reference knows only
+    its own softening, eps = epsMult sqrt(G max(m1, m2) dt); epsMult is set so
+    that eps equals the workload's Plummer eps at the median body mass."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    if not orc.ref_available():
+        return None
+    cfg = wl["config"]
+    n = wl["n"]
+    mass, pos, vel, _ = pkg.generate_scenario(wl["scenario"], n, 1, cfg.gravConstant)
+    m_med = float(np.median(mass))
+    eps_mult = float(cfg.plummerEps / np.sqrt(cfg.gravConstant * m_med * cfg.deltaTime))
+    kw = dict(G=cfg.gravConstant, dt=cfg.deltaTime, eps_mult=eps_mult, theta=cfg.bhTheta,
+              parallel=True)
+    t0 = time.perf_counter()
+    orc.ref_run(mass, pos, vel, steps=1, **kw)  # warm-up and size the sample
+    one = time.perf_counter() - t0
+    steps = int(max(1, min(50, seconds_budget / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    orc.ref_run(mass, pos, vel, steps=steps, **kw)
+    el = time.perf_counter() - t0
+    threads = orc.ref_threads()
+    return {"value": n * steps / el, "unit": "body-steps/s", "cores": threads, "kind": "reference",
+            "sample": f"{steps} steps of the full {n}-body workload (reference WGSL logic "
+                      f"translated to C++, fixed 2000-unit Morton domain, per-body monopole walk, "
+                      f"epsMult {eps_mult:.1f}, {threads} OpenMP threads; fill serial)"}
+
+
 def cpu_baseline(pkg, wl, seconds_budget=20.0):
+    """The reference's own logic when it was built here, else the oracle port."""
+    ref = reference_baseline(pkg, wl, seconds_budget)
+    return ref if ref is not None else port_baseline(pkg, wl, seconds_budget)
+
+
+def port_baseline(pkg, wl, seconds_budget=20.0):
     """The oracle (C restatement, OpenMP) on a bounded sample of the workload."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc

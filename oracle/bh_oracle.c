@@ -216,7 +216,9 @@ void orc_build(uint32_t n, int morton_bits, const uint64_t* k, uint32_t* left, u
     if (n == 0) return;
     const int64_t N = n;
     const int bits = morton_bits;
-    parent[0] = 0xFFFFFFFFu; /* lbvh.wgsl:159-161; for n == 1 the root is the only leaf */
+    /* n == 1: build_lbvh_main has no internal node to run (lbvh.wgsl:95-97),
+     * so the only node keeps the zero-initialised parent of its buffer. */
+    if (n == 1) parent[0] = 0u;
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < N - 1; ++i) {
         int d = delta_fn(k, N, bits, i, i + 1) > delta_fn(k, N, bits, i, i - 1) ? 1 : -1;
@@ -475,7 +477,8 @@ void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const 
     uint32_t* first = (uint32_t*)malloc(sizeof(uint32_t) * (2 * (size_t)n - 1));
     uint32_t* last = (uint32_t*)malloc(sizeof(uint32_t) * (2 * (size_t)n - 1));
     node_ranges(n, left, right, first, last);
-    /* Groups: maximal subtrees of <= G bodies (contiguous slots of one cell). */
+    /* Groups: the maximal subtrees of <= 2G bodies (contiguous slots of one
+     * cell), cut into runs of G slots. */
     uint32_t* gfirst = (uint32_t*)malloc(sizeof(uint32_t) * n);
     uint32_t* gcount = (uint32_t*)malloc(sizeof(uint32_t) * n);
     uint32_t ngroups = 0;
@@ -486,9 +489,13 @@ void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const 
         while (sp > 0) {
             const uint32_t v = st[--sp];
             const uint32_t c = last[v] - first[v] + 1;
-            if (c <= G) {
+            if (c <= 2 * G) {
                 gfirst[ngroups] = first[v];
-                gcount[ngroups++] = c;
+                gcount[ngroups++] = c <= G ? c : G;
+                if (c > G) {
+                    gfirst[ngroups] = first[v] + G;
+                    gcount[ngroups++] = c - G;
+                }
             } else {
                 st[sp++] = right[v];
                 st[sp++] = left[v];

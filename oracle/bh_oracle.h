@@ -96,8 +96,9 @@ void orc_walk(const orc_params* p, uint32_t n, const uint32_t* ids, const float*
 void orc_quadrupoles(uint32_t n, const uint32_t* left, const uint32_t* right, const float* com,
                      const float* mass_node, float* quad);
 
-/* Extension: group walk.  Groups are the maximal subtrees of at most
- * 32*bodies_per_lane bodies (contiguous sorted slots); a group opens a node unless L^2 < theta^2 d^2 (L = longest side of the node's
+/* Extension: group walk.  Groups are runs of at most G = 32*bodies_per_lane
+ * sorted slots cut from the maximal subtrees of at most 2G bodies; a group
+ * opens a node unless L^2 < theta^2 d^2 (L = longest side of the node's
  * box, d = distance between the group's box and the node's box); accepted
  * nodes act through monopole (+ quadrupole), leaves and opened nodes of
  * <= leaf_size bodies body by body.  acc[2*body]. */

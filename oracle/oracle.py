@@ -196,6 +196,58 @@ def direct_sum_fp64(p: OrcParams, mass, pos, sample) -> np.ndarray:
     return out
 
 
+REF_LIB = os.path.join(HERE, "_ref", "libref_wgsl.so")
+_ref = None
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def _ref_lib():
+    global _ref
+    if _ref is None:
+        lib = ctypes.CDLL(REF_LIB)
+        lib.ref_run.restype = ctypes.c_int
+        lib.ref_run.argtypes = [ctypes.c_uint32, _P, _P, _P, ctypes.c_float, ctypes.c_float,
+                                ctypes.c_float, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32,
+                                ctypes.c_int] + [_P] * 11
+        lib.ref_max_threads.restype = ctypes.c_int
+        lib.ref_max_threads.argtypes = []
+        _ref = lib
+    return _ref
+
+
+def ref_threads() -> int:
+    return _ref_lib().ref_max_threads()
+
+
+def ref_run(mass, pos, vel, G=1.0, dt=0.1 / 60.0, eps_mult=1.0, theta=0.6, offset=0, steps=1,
+            parallel=False):
+    """Run the mechanically translated reference WGSL (oracle/_ref) for
+    `steps` steps; returns the final state and the last step's tree.
+    parallel=True runs the independent stages on all host threads (same
+    results)."""
+    _ref_lib()
+    mass = f32(mass)
+    pos = f32(pos, (-1, 2))
+    vel = f32(vel, (-1, 2))
+    n = mass.size
+    nn = max(2 * n - 1, 1)
+    out = dict(pos=np.zeros((n, 2), np.float32), vel=np.zeros((n, 2), np.float32),
+               codes=np.zeros(n, np.uint32), ids=np.zeros(n, np.uint32),
+               left=np.zeros(nn, np.uint32), right=np.zeros(nn, np.uint32),
+               parent=np.zeros(nn, np.uint32), com=np.zeros((nn, 2), np.float32),
+               mass=np.zeros(nn, np.float32), aabb=np.zeros((nn, 4), np.float32),
+               length=np.zeros(nn, np.float32))
+    _ref.ref_run(n, _p(mass), _p(pos), _p(vel), G, dt, eps_mult, theta, offset, steps,
+                 1 if parallel else 0,
+                 _p(out["pos"]), _p(out["vel"]), _p(out["codes"]), _p(out["ids"]), _p(out["left"]),
+                 _p(out["right"]), _p(out["parent"]), _p(out["com"]), _p(out["mass"]),
+                 _p(out["aabb"]), _p(out["length"]))
+    return out
+
+
 class State:
     """Whole-step oracle run (simulation.ts:386-425 stage order)."""
 

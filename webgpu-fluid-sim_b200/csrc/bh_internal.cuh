@@ -43,6 +43,7 @@ struct __align__(16) GNode {
 constexpr int kGroupStack = 1024;
 constexpr int kGroupDfsAt = kGroupStack - 128;  // switch to one node per step above this depth
 constexpr int kGroupList = 64;
+constexpr int kGroupMaxLeaf = 8;                // leaf_size cap of the group walk
 constexpr uint32_t kErrGroupStack = 1u << 3;    // group-walk stack overflow (never expected)
 
 // Walk modes.

@@ -111,6 +111,8 @@ static int validate_config(bh_sim* s, const bh_config& c) {
     if (c.substeps < 1) return fail(s, BH_ERR_INVALID_ARGUMENT, "substeps must be >= 1");
     if (c.leaf_size < 1 || c.leaf_size > 64)
         return fail(s, BH_ERR_INVALID_ARGUMENT, "leaf_size must be in [1, 64]");
+    if (c.walk_mode == BH_WALK_GROUP && c.leaf_size > bh::kGroupMaxLeaf)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "leaf_size must be <= 8 with the group walk");
     if (c.walk_mode != BH_WALK_EXACT && c.walk_mode != BH_WALK_GROUP)
         return fail(s, BH_ERR_INVALID_ARGUMENT, "unknown walk_mode");
     if (c.walk_mode == BH_WALK_GROUP && c.multipole_order != 1 && c.multipole_order != 2)

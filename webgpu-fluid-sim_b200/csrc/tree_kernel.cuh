@@ -20,17 +20,19 @@
 // left/right/parent arrays as the reference's top-down build, bit for bit.
 //
 // Synchronisation: the two children of a split gamma meet at bound[gamma] with
-// an atomic exchange of their far range ends; the first arriver stops.  Node
-// records are published with __threadfence() before the exchange and read by
-// the second arriver through L2 (__ldcg) after it, so no stale data is ever
-// combined.  There are no spins.  bound[] holds kSentinel between steps: the
-// second arriver restores it.
+// an atomic exchange of their far range ends; the first arriver stops.  The
+// exchange is acq_rel at device scope: it releases the node record this
+// thread wrote and acquires the sibling's, which the second arriver then reads
+// through L2 (__ldcg), so no stale data is ever combined.  There are no spins.
+// bound[] holds kSentinel between steps: the second arriver restores it.
 //
 // Mass / COM: small nodes use the reference's f32 formula
 //   M = m_l + m_r;  com = (c_l m_l + c_r m_r) / M  (0 if M <= 0)   (lbvh.wgsl:216-224)
 // and nodes of >= kFp64MinBodies bodies aggregate {m, m x, m y} in FP64.
 // AABB and length = longest side are exact (lbvh.wgsl:212-213,227-228).
 #pragma once
+
+#include <cuda/atomic>
 
 #include "bh_internal.cuh"
 
@@ -62,7 +64,9 @@ build_fill_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ ids,
     const float2 p = __ldg(&pos[body]);
     node4[nm1 + i] = make_float4(p.x, p.y, m, 0.0f);  // leaf (lbvh.wgsl:179-187)
     if (n == 1) {
-        parent[0] = kSentinel;
+        // The reference's build has no internal node to run for n == 1
+        // (lbvh.wgsl:95-97): the only node keeps its buffer's initial 0.
+        parent[0] = 0u;
         if (groups) {
             groups[0] = make_uint2(0u, 1u);
             *group_count = 1u;
@@ -75,16 +79,19 @@ build_fill_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ ids,
     double dm = 0.0, dmx = 0.0, dmy = 0.0;  // valid when the node has >= kFp64MinBodies bodies
     float sxx = 0.0f, sxy = 0.0f, syy = 0.0f;  // second moments about the COM (group walk)
     uint32_t l = i, r = i;
+    // delta at the two boundaries of the current range (-1 outside [0, n-1]);
+    // a parent keeps one of them, so each level computes only one new delta.
+    int dl = (l == 0) ? -1 : delta_at(keys, l - 1, l);
+    int dr = (r == nm1) ? -1 : delta_at(keys, r, r + 1);
     while (true) {
-        const int dl = (l == 0) ? -1 : delta_at(keys, l - 1, l);
-        const int dr = (r == nm1) ? -1 : delta_at(keys, r, r + 1);
         const bool is_left = dr > dl;
         const uint32_t gamma = is_left ? r : l - 1;
-        __threadfence();
-        const uint32_t other = atomicExch(&bound[gamma], is_left ? l : r);
+        // One acq_rel exchange releases this node's record and acquires the
+        // sibling's (release/acquire through bound[gamma]).
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> slot(bound[gamma]);
+        const uint32_t other = slot.exchange(is_left ? l : r, cuda::memory_order_acq_rel);
         if (other == kSentinel) return;  // first to arrive: the sibling finishes the parent
-        __threadfence();
-        bound[gamma] = kSentinel;
+        slot.store(kSentinel, cuda::memory_order_relaxed);
         const uint32_t pl = is_left ? l : other;
         const uint32_t pr = is_left ? other : r;
         const uint32_t li = (pl == gamma) ? nm1 + gamma : gamma;
@@ -92,22 +99,34 @@ build_fill_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ ids,
         const uint32_t sib = is_left ? ri : li;
         const uint32_t sib_cnt = is_left ? (pr - gamma) : (gamma - pl + 1);
         const uint32_t my_cnt = r - l + 1;
-        const float4 s4 = __ldcg(&node4[sib]);
-        const float4 sb = (sib >= nm1) ? make_float4(s4.x, s4.y, s4.x, s4.y) : __ldcg(&aabb[sib]);
+        // Sibling record through L2 (written by another thread in this launch).
+        float4 s4, sb, sq = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (sib >= nm1) {
+            s4 = __ldcg(&node4[sib]);
+            sb = make_float4(s4.x, s4.y, s4.x, s4.y);
+        } else if (gnode) {
+            sb = __ldcg(&gnode[sib].box);
+            s4 = __ldcg(&gnode[sib].mom);
+            sq = __ldcg(&gnode[sib].quad);
+        } else {
+            s4 = __ldcg(&node4[sib]);
+            sb = __ldcg(&aabb[sib]);
+        }
         lox = fminf(lox, sb.x);
         loy = fminf(loy, sb.y);
         hix = fmaxf(hix, sb.z);
         hiy = fmaxf(hiy, sb.w);
         const uint32_t cnt = pr - pl + 1;
-        // Parent's own Karras index.
-        uint32_t pidx;
-        if (pl == 0 && pr == nm1) {
-            pidx = 0;
+        // Parent's boundary deltas and its own Karras index.
+        int dpl, dpr;
+        if (is_left) {
+            dpl = dl;
+            dpr = (pr == nm1) ? -1 : delta_at(keys, pr, pr + 1);
         } else {
-            const int dpl = (pl == 0) ? -1 : delta_at(keys, pl - 1, pl);
-            const int dpr = (pr == nm1) ? -1 : delta_at(keys, pr, pr + 1);
-            pidx = (dpr > dpl) ? pr : pl;
+            dpr = dr;
+            dpl = (pl == 0) ? -1 : delta_at(keys, pl - 1, pl);
         }
+        const uint32_t pidx = (pl == 0 && pr == nm1) ? 0u : ((dpr > dpl) ? pr : pl);
         float tm, ncx, ncy;
         if (fp64 && cnt >= kFp64MinBodies) {
             double sm, smx, smy;
@@ -146,8 +165,6 @@ build_fill_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ ids,
         if (gnode) {
             // Second moments about the parent COM, left child first:
             // S = sum_c S_c + m_c d_c d_c^T, d_c = c_c - c_parent (leaves: S_c = 0).
-            float4 sq = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (sib < nm1) sq = __ldcg(&gnode[sib].quad);
             float ml, mr, lxx, lxy, lyy, rxx, rxy, ryy, dlx, dly, drx, dry;
             if (is_left) {
                 ml = cm; lxx = sxx; lxy = sxy; lyy = syy; dlx = __fsub_rn(cx, ncx); dly = __fsub_rn(cy, ncy);
@@ -170,14 +187,25 @@ build_fill_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ ids,
             gnode[pidx] = g;
         }
         if (groups) {
-            // Walk groups: maximal subtrees of <= gmax bodies.  A child is one
-            // when its parent is too big; the whole tree is one when n <= gmax.
-            if (cnt > gmax) {
+            // Walk groups: the maximal subtrees of <= 2 gmax bodies, cut into
+            // runs of gmax slots (a child is such a subtree when its parent is
+            // bigger; the whole tree is one when n <= 2 gmax).
+            const uint32_t gsub = 2u * gmax;
+            auto emit = [&](uint32_t f, uint32_t c) {
+                if (c <= gmax) {
+                    groups[atomicAdd(group_count, 1u)] = make_uint2(f, c);
+                } else {
+                    const uint32_t at = atomicAdd(group_count, 2u);
+                    groups[at] = make_uint2(f, gmax);
+                    groups[at + 1] = make_uint2(f + gmax, c - gmax);
+                }
+            };
+            if (cnt > gsub) {
                 const uint32_t lcnt = gamma - pl + 1, rcnt = pr - gamma;
-                if (lcnt <= gmax) groups[atomicAdd(group_count, 1u)] = make_uint2(pl, lcnt);
-                if (rcnt <= gmax) groups[atomicAdd(group_count, 1u)] = make_uint2(gamma + 1, rcnt);
+                if (lcnt <= gsub) emit(pl, lcnt);
+                if (rcnt <= gsub) emit(gamma + 1, rcnt);
             } else if (pidx == 0) {
-                groups[atomicAdd(group_count, 1u)] = make_uint2(0u, n);
+                emit(0u, n);
             }
         }
         node4[pidx] = make_float4(ncx, ncy, tm, len);
@@ -193,6 +221,8 @@ build_fill_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ ids,
         cm = tm; cx = ncx; cy = ncy;
         l = pl;
         r = pr;
+        dl = dpl;
+        dr = dpr;
     }
 }
 

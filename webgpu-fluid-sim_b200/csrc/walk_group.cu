@@ -6,11 +6,13 @@
 // walk has a median relative force error of order 1e-2 at theta = 0.5 in 2D;
 // this walk reaches <= 1e-3 at the same theta.
 //
-// One warp owns a group: a maximal subtree of at most 32 x BPL bodies, i.e.
-// contiguous sorted slots inside one Morton cell (listed by the build
-// kernel).  Fixed runs of 32 x BPL slots would not do: a run that straddles a
-// jump of the Z curve has a box spanning far-apart regions and opens nearly
-// every node.  The group opens a node unless
+// One warp owns a group: a run of at most G = 32 x BPL sorted slots cut from
+// a maximal subtree of at most 2G bodies, so its bodies lie inside one Morton
+// cell (the build kernel lists the groups).  Fixed runs of G slots over the
+// whole order would not do: a run that straddles a jump of the Z curve has a
+// box spanning far-apart regions and opens nearly every node; whole maximal
+// G-body subtrees would do but leave about 30% of the lanes idle.  The group
+// opens a node unless
 //     L^2 < theta^2 d^2,  L = longest side of the node's box,
 //     d = distance between the group's box and the node's box,
 // which is stricter for every body of the group than the per-body test
@@ -21,33 +23,85 @@
 // Leaves, and opened nodes of <= leaf_size bodies, are summed body by body.
 //
 // Traversal: a per-warp stack in shared memory.  Every step each lane takes
-// one of the top 32 stack entries, evaluates its node, and the warp compacts
-// the outcomes with ballots into a node list, a body-range list and the
-// stack.  Lists are evaluated when they hold >= 32 entries: every lane runs
-// every entry for its BPL bodies (shared-memory broadcasts, no divergence).
+// one of the top 32 stack entries, loads its whole 64-B record in one round
+// trip, evaluates it, and the warp compacts the outcomes (ballots and a
+// warp scan) into a node list, a body-slot list and the stack.  Lists are
+// evaluated when they hold >= 32 entries: every lane runs every entry for its
+// BPL bodies (shared-memory broadcasts, no divergence); body records are
+// first loaded 32 at a time by the 32 lanes in parallel.
 // Above kGroupDfsAt entries the warp pops one node per step (plain DFS), which
 // keeps the stack below kGroupStack for any tree of depth <= 96; a push that
 // would not fit raises kErrGroupStack instead of writing out of bounds.
 // Groups are taken from an atomic counter (the walk is persistent).
+//
+// Packed arithmetic: with BPL >= 2 each lane evaluates its bodies in pairs
+// with the sm_100 packed FP32 instructions (add/sub/mul/fma .rn.f32x2), one
+// instruction for both bodies.  Node-list entries are stored in shared memory
+// with every value duplicated ({cx,cx,cy,cy}, ...), so a 128-bit shared load
+// yields ready operand pairs, and with the quadrupole negated so every
+// accumulation is a plain fused multiply-add.  With eps^2 > 0 a body's own
+// leaf adds exactly zero (r = 0), so no self test is needed.
 #include "bh_internal.cuh"
 
 namespace bh {
 
 constexpr int kGroupWarps = 4;
+constexpr int kWalkStack = 384;               // per-warp stack entries
+constexpr int kWalkDfsAt = kWalkStack - 128;  // >= 32 + 96 below the capacity
+
+constexpr int kSlotList = 32 + 32 * kGroupMaxLeaf;  // body slots: < 32 kept + one step's adds
 
 struct GroupSmem {
-    uint32_t stack[kGroupStack];
-    float4 mom[kGroupList];   // {com.x, com.y, mass, 0}
-    float4 quad[kGroupList];  // {Q'xx, Q'xy, Q'yy, 0}
-    uint2 range[kGroupList];  // {first slot, count}
+    uint32_t stack[kWalkStack];
+    // node entry j: ent[j][0] = {cx, cx, cy, cy}, ent[j][1] = {m, m, -Q'xx, -Q'xx},
+    //               ent[j][2] = {-Q'xy, -Q'xy, -Q'yy, -Q'yy}
+    float4 ent[kGroupList][3];
+    uint32_t slot[kSlotList];  // sorted slots of bodies to sum one by one
+    float4 body[32][2];        // 32 staged leaf records as pairs {x,x,y,y}, {m,m,0,0}
 };
 
+// ---- packed FP32 pairs (sm_100 .f32x2) ----------------------------------------
+typedef unsigned long long f2x;
+__device__ __forceinline__ f2x pk(float lo, float hi) {
+    f2x r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk(f2x v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2x sub2(f2x a, f2x b) {
+    f2x r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2x mul2(f2x a, f2x b) {
+    f2x r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2x fma2(f2x a, f2x b, f2x c) {
+    f2x r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+__device__ __forceinline__ f2x rsqrt2(f2x v) {
+    float lo, hi;
+    upk(v, lo, hi);
+    return pk(rsqrtf(lo), rsqrtf(hi));
+}
+__device__ __forceinline__ f2x ld_pair(const float4& v, int half) {
+    // {v.x, v.y} or {v.z, v.w} of a shared-memory float4 as one 64-bit pair
+    return reinterpret_cast<const f2x*>(&v)[half];
+}
+
 template <int BPL, int MP, bool PLUMMER>
-__global__ void __launch_bounds__(kGroupWarps * 32)
+__global__ void __launch_bounds__(kGroupWarps * 32, 8)
 walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ node4,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ ids,
                   float2* __restrict__ pos, float2* __restrict__ vel, float2* __restrict__ acc,
                   const WalkParams P, uint32_t* __restrict__ err) {
+    constexpr int NP = BPL / 2;  // packed pairs per lane (BPL >= 2)
     __shared__ GroupSmem smem[kGroupWarps];
     const int lane = threadIdx.x & 31;
     GroupSmem& S = smem[threadIdx.x >> 5];
@@ -57,6 +111,8 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
     const uint32_t ngroups = P.group_ctr[1];  // written by the build kernel
     const float th2 = __fmul_rn(P.theta, P.theta);
     const float eps2 = P.eps2, ecoef = P.eps_coef;
+    // With a positive softening the own-leaf term is exactly zero.
+    const bool self_test = !(PLUMMER && eps2 > 0.0f);
     const bool counting = P.count != 0;
     unsigned long long c_vis = 0, c_node = 0, c_body = 0;
 
@@ -70,19 +126,17 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
         const uint2 grp = __ldg(&groups[g]);
         const uint32_t base = grp.x, nvalid = grp.y;
         const int kmax = (int)((nvalid + 31u) / 32u);  // sub-slots in use (uniform)
-        float bx[BPL], by[BPL], bm[BPL], ax[BPL], ay[BPL];
+        float bx[BPL], by[BPL], bm[BPL];
         float glox = INFINITY, gloy = INFINITY, ghix = -INFINITY, ghiy = -INFINITY;
 #pragma unroll
         for (int k = 0; k < BPL; ++k) {
-            const uint32_t s = base + (uint32_t)k * 32u + (uint32_t)lane;
             float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
             if ((uint32_t)k * 32u + (uint32_t)lane < nvalid) {
-                r = __ldg(&node4[nm1 + s]);
+                r = __ldg(&node4[nm1 + base + (uint32_t)k * 32u + (uint32_t)lane]);
                 glox = fminf(glox, r.x); gloy = fminf(gloy, r.y);
                 ghix = fmaxf(ghix, r.x); ghiy = fmaxf(ghiy, r.y);
             }
             bx[k] = r.x; by[k] = r.y; bm[k] = r.z;
-            ax[k] = 0.f; ay[k] = 0.f;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -91,62 +145,126 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
             ghix = fmaxf(ghix, __shfl_xor_sync(FULL, ghix, o));
             ghiy = fmaxf(ghiy, __shfl_xor_sync(FULL, ghiy, o));
         }
+        // Accumulators: packed pairs (BPL >= 2) or scalars (BPL == 1).
+        f2x X[NP > 0 ? NP : 1], Y[NP > 0 ? NP : 1], AX[NP > 0 ? NP : 1], AY[NP > 0 ? NP : 1];
+        float ax1 = 0.f, ay1 = 0.f;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            X[q] = pk(bx[2 * q], bx[2 * q + 1]);
+            Y[q] = pk(by[2 * q], by[2 * q + 1]);
+            AX[q] = pk(0.f, 0.f);
+            AY[q] = pk(0.f, 0.f);
+        }
+        const f2x E2 = pk(eps2, eps2);
+        const f2x M25 = pk(-2.5f, -2.5f);
 
-        // Evaluate the node list (multipoles) for this lane's bodies.
+        auto soft_pair = [&](int q, float m2) -> f2x {
+            if (PLUMMER) return E2;
+            return pk(ecoef * fmaxf(bm[2 * q], m2), ecoef * fmaxf(bm[2 * q + 1], m2));
+        };
+
+        // Node list: multipole interactions.
         auto eval_nodes = [&](int cnt) {
 #pragma unroll 2
             for (int j = 0; j < cnt; ++j) {
-                const float4 a = S.mom[j];
-                float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (MP >= 2) q = S.quad[j];
+                const float4 e0 = S.ent[j][0], e1 = S.ent[j][1];
+                float4 e2 = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (MP >= 2) e2 = S.ent[j][2];
+                if (NP > 0) {
+                    const f2x CX = ld_pair(e0, 0), CY = ld_pair(e0, 1), M = ld_pair(e1, 0);
 #pragma unroll
-                for (int k = 0; k < BPL; ++k) {
-                    if (k >= kmax) break;
-                    const float rx = a.x - bx[k], ry = a.y - by[k];
-                    const float e2 = PLUMMER ? eps2 : ecoef * fmaxf(bm[k], a.z);
-                    const float r2 = fmaf(rx, rx, fmaf(ry, ry, e2));
-                    const float inv = rsqrtf(r2);
-                    const float inv2 = inv * inv;
-                    const float inv3 = inv * inv2;
+                    for (int q = 0; q < NP; ++q) {
+                        if (2 * q >= kmax) break;
+                        const f2x rx = sub2(CX, X[q]), ry = sub2(CY, Y[q]);
+                        const f2x r2 = fma2(rx, rx, fma2(ry, ry, soft_pair(q, e1.x)));
+                        const f2x inv = rsqrt2(r2);
+                        const f2x inv2 = mul2(inv, inv);
+                        const f2x inv3 = mul2(inv, inv2);
+                        if (MP >= 2) {
+                            const f2x NQXX = ld_pair(e1, 1), NQXY = ld_pair(e2, 0), NQYY = ld_pair(e2, 1);
+                            const f2x nqrx = fma2(NQXX, rx, mul2(NQXY, ry));  // -(Q'r)_x
+                            const f2x nqry = fma2(NQXY, rx, mul2(NQYY, ry));  // -(Q'r)_y
+                            const f2x nrqr = fma2(rx, nqrx, mul2(ry, nqry)); // -r.Q'r
+                            const f2x inv5 = mul2(inv3, inv2);
+                            // f = (m + 5/2 r.Q'r / |r|^2) / |r|^3
+                            const f2x f = mul2(inv3, fma2(nrqr, mul2(M25, inv2), M));
+                            AX[q] = fma2(nqrx, inv5, fma2(f, rx, AX[q]));
+                            AY[q] = fma2(nqry, inv5, fma2(f, ry, AY[q]));
+                        } else {
+                            const f2x mi3 = mul2(M, inv3);
+                            AX[q] = fma2(mi3, rx, AX[q]);
+                            AY[q] = fma2(mi3, ry, AY[q]);
+                        }
+                    }
+                } else {
+                    const float rx = e0.x - bx[0], ry = e0.z - by[0];
+                    const float es = PLUMMER ? eps2 : ecoef * fmaxf(bm[0], e1.x);
+                    const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, es)));
+                    const float inv2 = inv * inv, inv3 = inv * inv2;
+                    const float mi3 = e1.x * inv3;
                     if (MP >= 2) {
-                        const float qrx = fmaf(q.x, rx, q.y * ry);
-                        const float qry = fmaf(q.y, rx, q.z * ry);
-                        const float rqr = fmaf(rx, qrx, ry * qry);
+                        const float nqrx = fmaf(e1.z, rx, e2.x * ry);
+                        const float nqry = fmaf(e2.x, rx, e2.z * ry);
+                        const float nrqr = fmaf(rx, nqrx, ry * nqry);
                         const float inv5 = inv3 * inv2;
-                        const float f = fmaf(2.5f * rqr, inv5 * inv2, a.z * inv3);
-                        ax[k] = fmaf(-qrx, inv5, fmaf(f, rx, ax[k]));
-                        ay[k] = fmaf(-qry, inv5, fmaf(f, ry, ay[k]));
+                        const float f = fmaf(-2.5f * nrqr, inv5 * inv2, mi3);
+                        ax1 = fmaf(nqrx, inv5, fmaf(f, rx, ax1));
+                        ay1 = fmaf(nqry, inv5, fmaf(f, ry, ay1));
                     } else {
-                        const float f = a.z * inv3;
-                        ax[k] = fmaf(f, rx, ax[k]);
-                        ay[k] = fmaf(f, ry, ay[k]);
+                        ax1 = fmaf(mi3, rx, ax1);
+                        ay1 = fmaf(mi3, ry, ay1);
                     }
                 }
             }
         };
-        // Evaluate the body-range list (point masses, own slot skipped).
-        auto eval_ranges = [&](int cnt) {
-            for (int j = 0; j < cnt; ++j) {
-                const uint2 rg = S.range[j];
-                for (uint32_t s = rg.x; s < rg.x + rg.y; ++s) {
-                    const float4 o = __ldg(&node4[nm1 + s]);
+        // Body list: point masses.  32 leaf records at a time are loaded by the
+        // 32 lanes in parallel into shared memory, then every lane sums them.
+        auto eval_bodies = [&](int cnt) {
+            for (int c0 = 0; c0 < cnt; c0 += 32) {
+                const int mcnt = (cnt - c0) < 32 ? (cnt - c0) : 32;
+                __syncwarp();
+                if (lane < mcnt) {
+                    const float4 o = __ldg(&node4[nm1 + S.slot[c0 + lane]]);
+                    S.body[lane][0] = make_float4(o.x, o.x, o.y, o.y);
+                    S.body[lane][1] = make_float4(o.z, o.z, 0.f, 0.f);
+                }
+                __syncwarp();
+                for (int j = 0; j < mcnt; ++j) {
+                    const float4 p0 = S.body[j][0], p1 = S.body[j][1];
+                    const uint32_t s = self_test ? S.slot[c0 + j] : 0u;
+                    if (NP > 0) {
+                        const f2x OX = ld_pair(p0, 0), OY = ld_pair(p0, 1), OM = ld_pair(p1, 0);
 #pragma unroll
-                    for (int k = 0; k < BPL; ++k) {
-                        if (k >= kmax) break;
-                        const float rx = o.x - bx[k], ry = o.y - by[k];
-                        const float e2 = PLUMMER ? eps2 : ecoef * fmaxf(bm[k], o.z);
-                        const float r2 = fmaf(rx, rx, fmaf(ry, ry, e2));
-                        const float inv = rsqrtf(r2);
-                        float f = o.z * (inv * inv * inv);
-                        f = (s == base + (uint32_t)k * 32u + (uint32_t)lane) ? 0.0f : f;
-                        ax[k] = fmaf(f, rx, ax[k]);
-                        ay[k] = fmaf(f, ry, ay[k]);
+                        for (int q = 0; q < NP; ++q) {
+                            if (2 * q >= kmax) break;
+                            const f2x rx = sub2(OX, X[q]), ry = sub2(OY, Y[q]);
+                            const f2x r2 = fma2(rx, rx, fma2(ry, ry, soft_pair(q, p1.x)));
+                            const f2x inv = rsqrt2(r2);
+                            f2x f = mul2(OM, mul2(inv, mul2(inv, inv)));
+                            if (self_test) {
+                                const uint32_t s0 = base + (uint32_t)(2 * q) * 32u + (uint32_t)lane;
+                                float f0, f1;
+                                upk(f, f0, f1);
+                                f = pk(s == s0 ? 0.0f : f0, s == s0 + 32u ? 0.0f : f1);
+                            }
+                            AX[q] = fma2(f, rx, AX[q]);
+                            AY[q] = fma2(f, ry, AY[q]);
+                        }
+                    } else {
+                        const float rx = p0.x - bx[0], ry = p0.z - by[0];
+                        const float es = PLUMMER ? eps2 : ecoef * fmaxf(bm[0], p1.x);
+                        const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, es)));
+                        float f = p1.x * (inv * inv * inv);
+                        if (self_test) f = (s == base + (uint32_t)lane) ? 0.0f : f;
+                        ax1 = fmaf(f, rx, ax1);
+                        ay1 = fmaf(f, ry, ay1);
                     }
                 }
             }
+            __syncwarp();
         };
 
-        int sp = 0, nn = 0, nr = 0;
+        int sp = 0, nn = 0, ns = 0;
         if (n > 1) {
             if (lane == 0) S.stack[0] = 0u;
             sp = 1;
@@ -154,7 +272,7 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
         __syncwarp();
         while (sp > 0) {
             int k = sp < 32 ? sp : 32;
-            if (sp > kGroupDfsAt) k = 1;
+            if (sp > kWalkDfsAt) k = 1;
             const bool has = lane < k;
             const uint32_t v = has ? S.stack[sp - k + lane] : 0u;
             sp -= k;
@@ -168,45 +286,63 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
                     r0 = v - nm1;
                     r1 = 1;
                 } else {
-                    const float4 box = __ldg(&gnode[v].box);
+                    // the whole 64-B record in one round trip
+                    const GNode* gp = &gnode[v];
+                    const float4 box = __ldg(&gp->box);
+                    const float4 m4 = __ldg(&gp->mom);
+                    const float4 q4 = __ldg(&gp->quad);
+                    const uint4 lk = __ldg(&gp->link);
                     const float dx = fmaxf(0.0f, fmaxf(__fsub_rn(box.x, ghix), __fsub_rn(glox, box.z)));
                     const float dy = fmaxf(0.0f, fmaxf(__fsub_rn(box.y, ghiy), __fsub_rn(gloy, box.w)));
                     const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
                     const float L = fmaxf(__fsub_rn(box.z, box.x), __fsub_rn(box.w, box.y));
                     if (__fmul_rn(L, L) < __fmul_rn(th2, d2)) {
                         emit_node = true;
-                        mom = __ldg(&gnode[v].mom);
-                        if (MP >= 2) sq = __ldg(&gnode[v].quad);
+                        mom = m4;
+                        sq = q4;
+                    } else if (lk.w <= (uint32_t)P.leaf_size) {
+                        emit_range = true;
+                        r0 = lk.z;
+                        r1 = lk.w;
                     } else {
-                        const uint4 lk = __ldg(&gnode[v].link);
-                        if (lk.w <= (uint32_t)P.leaf_size) {
-                            emit_range = true;
-                            r0 = lk.z;
-                            r1 = lk.w;
-                        } else {
-                            push = true;
-                            r0 = lk.x;
-                            r1 = lk.y;
-                        }
+                        push = true;
+                        r0 = lk.x;
+                        r1 = lk.y;
                     }
                 }
             }
             const unsigned mn = __ballot_sync(FULL, emit_node);
             if (emit_node) {
                 const int p = nn + __popc(mn & lt);
-                S.mom[p] = make_float4(mom.x, mom.y, mom.z, 0.0f);
+                S.ent[p][0] = make_float4(mom.x, mom.x, mom.y, mom.y);
                 if (MP >= 2) {
+                    // -Q' = tr(S) I - 3S
                     const float tr = sq.x + sq.z;
-                    S.quad[p] = make_float4(3.0f * sq.x - tr, 3.0f * sq.y, 3.0f * sq.z - tr, 0.0f);
+                    const float nxx = tr - 3.0f * sq.x, nxy = -3.0f * sq.y, nyy = tr - 3.0f * sq.z;
+                    S.ent[p][1] = make_float4(mom.z, mom.z, nxx, nxx);
+                    S.ent[p][2] = make_float4(nxy, nxy, nyy, nyy);
+                } else {
+                    S.ent[p][1] = make_float4(mom.z, mom.z, 0.f, 0.f);
                 }
             }
             nn += __popc(mn);
-            const unsigned mr = __ballot_sync(FULL, emit_range);
-            if (emit_range) S.range[nr + __popc(mr & lt)] = make_uint2(r0, r1);
-            nr += __popc(mr);
+            {
+                // Append this step's body slots: exclusive scan of the counts.
+                const uint32_t c = emit_range ? r1 : 0u;
+                uint32_t incl = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const uint32_t total = __shfl_sync(FULL, incl, 31);
+                const uint32_t at = (uint32_t)ns + incl - c;
+                for (uint32_t u = 0; u < c; ++u) S.slot[at + u] = r0 + u;
+                ns += (int)total;
+            }
             const unsigned mp = __ballot_sync(FULL, push);
             const int npush = 2 * __popc(mp);
-            if (sp + npush <= kGroupStack) {
+            if (sp + npush <= kWalkStack) {
                 if (push) {
                     const int p = sp + 2 * __popc(mp & lt);
                     S.stack[p] = r1;      // right child
@@ -224,27 +360,35 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
                 nn = 0;
                 __syncwarp();
             }
-            if (nr >= 32) {
-                if (counting)
-                    for (int j = 0; j < nr; ++j) c_body += (unsigned long long)S.range[j].y * nvalid;
-                eval_ranges(nr);
-                nr = 0;
-                __syncwarp();
+            if (ns >= 32) {
+                if (counting) c_body += (unsigned long long)ns * nvalid;
+                eval_bodies(ns);
+                ns = 0;
             }
         }
         if (nn > 0) {
             eval_nodes(nn);
             if (counting) c_node += (unsigned long long)nn * nvalid;
         }
-        if (nr > 0) {
-            if (counting)
-                for (int j = 0; j < nr; ++j) c_body += (unsigned long long)S.range[j].y * nvalid;
-            eval_ranges(nr);
+        if (ns > 0) {
+            if (counting) c_body += (unsigned long long)ns * nvalid;
+            eval_bodies(ns);
         }
         if (counting && n > 1) c_body -= nvalid;  // each body met its own leaf once
         __syncwarp();
 
         // Integrate (same modes as the exact walk).
+        float ax[BPL], ay[BPL];
+        if (NP > 0) {
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                upk(AX[q], ax[2 * q], ax[2 * q + 1]);
+                upk(AY[q], ay[2 * q], ay[2 * q + 1]);
+            }
+        } else {
+            ax[0] = ax1;
+            ay[0] = ay1;
+        }
 #pragma unroll
         for (int k = 0; k < BPL; ++k) {
             const uint32_t s = base + (uint32_t)k * 32u + (uint32_t)lane;
@@ -254,18 +398,18 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
             if (P.mode == kWalkForces) {
                 acc[b] = make_float2(gx, gy);
             } else if (P.mode == kWalkEulerKickDrift) {
-                float2 v = vel[b];
-                v.x = __fadd_rn(v.x, __fmul_rn(gx, P.dt));
-                v.y = __fadd_rn(v.y, __fmul_rn(gy, P.dt));
-                vel[b] = v;
-                pos[b] = make_float2(__fadd_rn(bx[k], __fmul_rn(v.x, P.dt)),
-                                     __fadd_rn(by[k], __fmul_rn(v.y, P.dt)));
+                float2 vv = vel[b];
+                vv.x = __fadd_rn(vv.x, __fmul_rn(gx, P.dt));
+                vv.y = __fadd_rn(vv.y, __fmul_rn(gy, P.dt));
+                vel[b] = vv;
+                pos[b] = make_float2(__fadd_rn(bx[k], __fmul_rn(vv.x, P.dt)),
+                                     __fadd_rn(by[k], __fmul_rn(vv.y, P.dt)));
             } else {
                 const float hdt = 0.5f * P.dt;
-                float2 v = vel[b];
-                v.x = __fadd_rn(v.x, __fmul_rn(gx, hdt));
-                v.y = __fadd_rn(v.y, __fmul_rn(gy, hdt));
-                vel[b] = v;
+                float2 vv = vel[b];
+                vv.x = __fadd_rn(vv.x, __fmul_rn(gx, hdt));
+                vv.y = __fadd_rn(vv.y, __fmul_rn(gy, hdt));
+                vel[b] = vv;
                 acc[b] = make_float2(gx, gy);
             }
         }
