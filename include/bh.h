@@ -192,6 +192,28 @@ int bh_kernels_per_step(bh_sim* sim, uint32_t* out);
 int bh_walk_stats(bh_sim* sim, uint64_t* node_visits, uint64_t* multipole_interactions,
                   uint64_t* body_interactions);
 
+/* ---- differentiation (extension; no reference counterpart) ---------------- */
+/* Vector-Jacobian product of the force at the current positions: given
+ * abar[2n] (host), returns xbar[2n] = (da/dx)^T abar and mbar[n] =
+ * (da/dm)^T abar (host; either may be NULL).  The interaction lists are those
+ * of the forward group walk (topology held fixed), node moments are
+ * differentiated down to their member bodies.  Needs walk_mode
+ * BH_WALK_GROUP and Plummer softening (else BH_ERR_NOT_SUPPORTED). */
+int bh_force_vjp(bh_sim* sim, const float* abar, float* xbar, float* mbar);
+
+/* Differentiable rollout: advances `steps` kick-drift-kick steps from the
+ * current state, evaluates L = (1/n) sum_i |x_T,i - target_i|^2 and its
+ * gradient with respect to the initial positions, velocities and masses by
+ * a reverse sweep: positions and velocities are checkpointed every
+ * `checkpoint_every` steps, each segment is replayed (trees rebuilt) and the
+ * force VJP is applied once per force point.  The handle is left at step T.
+ * Host arrays: target_pos[2n]; outputs grad_pos[2n], grad_vel[2n],
+ * grad_mass[n] (any may be NULL).  Needs the leapfrog integrator, the group
+ * walk and Plummer softening. */
+int bh_rollout_grad(bh_sim* sim, uint32_t steps, uint32_t checkpoint_every,
+                    const float* target_pos, float* loss, float* grad_pos, float* grad_vel,
+                    float* grad_mass);
+
 /* ---- allocation-free hierarchy build ------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot let this library
  * allocate device memory (a host that plans the whole GPU heap and hands out

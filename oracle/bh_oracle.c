@@ -477,8 +477,7 @@ void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const 
     uint32_t* first = (uint32_t*)malloc(sizeof(uint32_t) * (2 * (size_t)n - 1));
     uint32_t* last = (uint32_t*)malloc(sizeof(uint32_t) * (2 * (size_t)n - 1));
     node_ranges(n, left, right, first, last);
-    /* Groups: the maximal subtrees of <= 2G bodies (contiguous slots of one
-     * cell), cut into runs of G slots. */
+    /* Groups: the maximal subtrees of <= G bodies (contiguous slots of one cell). */
     uint32_t* gfirst = (uint32_t*)malloc(sizeof(uint32_t) * n);
     uint32_t* gcount = (uint32_t*)malloc(sizeof(uint32_t) * n);
     uint32_t ngroups = 0;
@@ -489,13 +488,9 @@ void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const 
         while (sp > 0) {
             const uint32_t v = st[--sp];
             const uint32_t c = last[v] - first[v] + 1;
-            if (c <= 2 * G) {
+            if (c <= G) {
                 gfirst[ngroups] = first[v];
-                gcount[ngroups++] = c <= G ? c : G;
-                if (c > G) {
-                    gfirst[ngroups] = first[v] + G;
-                    gcount[ngroups++] = c - G;
-                }
+                gcount[ngroups++] = c;
             } else {
                 st[sp++] = right[v];
                 st[sp++] = left[v];
@@ -644,6 +639,137 @@ void orc_direct_sum_fp64(const orc_params* p, uint32_t n, const float* mass, con
         acc_out[2 * k] = ax;
         acc_out[2 * k + 1] = ay;
     }
+}
+
+/* ------------------------------------------------------------------------ */
+/* FP64 direct-sum rollout adjoint (no reference counterpart)                */
+/* ------------------------------------------------------------------------ */
+
+/* a_i = G sum_{j != i} m_j r_ij s_ij^3, r_ij = x_j - x_i, s = (r.r + eps^2)^-1/2 */
+static void ds_accel(int nt, uint32_t n, double G, double e2, const double* m, const double* x,
+                     double* a) {
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        double ax = 0.0, ay = 0.0;
+        for (uint32_t j = 0; j < n; ++j) {
+            if ((int64_t)j == i) continue;
+            double rx = x[2 * j] - x[2 * i], ry = x[2 * j + 1] - x[2 * i + 1];
+            double s = 1.0 / sqrt(rx * rx + ry * ry + e2);
+            double f = m[j] * s * s * s;
+            ax += f * rx;
+            ay += f * ry;
+        }
+        a[2 * i] = G * ax;
+        a[2 * i + 1] = G * ay;
+    }
+}
+
+/* (xbar, mbar) += (da/dx, da/dm)^T abar.  With rbar_ij = m_j (s^3 ab_i -
+ * 3 s^5 (ab_i.r) r): xbar_i -= sum_j rbar_ij, xbar_j += sum_i rbar_ij,
+ * mbar_j += sum_i s^3 (ab_i.r).  Two passes keep every write private. */
+static void ds_vjp(int nt, uint32_t n, double G, double e2, const double* m, const double* x,
+                   const double* ab, double* xbar, double* mbar) {
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        double bx = 0.0, by = 0.0;
+        const double ax = G * ab[2 * i], ay = G * ab[2 * i + 1];
+        for (uint32_t j = 0; j < n; ++j) {
+            if ((int64_t)j == i) continue;
+            double rx = x[2 * j] - x[2 * i], ry = x[2 * j + 1] - x[2 * i + 1];
+            double s = 1.0 / sqrt(rx * rx + ry * ry + e2), s3 = s * s * s, s5 = s3 * s * s;
+            double ar = ax * rx + ay * ry;
+            bx += m[j] * (s3 * ax - 3.0 * s5 * ar * rx);
+            by += m[j] * (s3 * ay - 3.0 * s5 * ar * ry);
+        }
+        xbar[2 * i] -= bx;
+        xbar[2 * i + 1] -= by;
+    }
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t j = 0; j < (int64_t)n; ++j) {
+        double bx = 0.0, by = 0.0, bm = 0.0;
+        for (uint32_t i = 0; i < n; ++i) {
+            if ((int64_t)i == j) continue;
+            const double ax = G * ab[2 * i], ay = G * ab[2 * i + 1];
+            double rx = x[2 * j] - x[2 * i], ry = x[2 * j + 1] - x[2 * i + 1];
+            double s = 1.0 / sqrt(rx * rx + ry * ry + e2), s3 = s * s * s, s5 = s3 * s * s;
+            double ar = ax * rx + ay * ry;
+            bx += m[j] * (s3 * ax - 3.0 * s5 * ar * rx);
+            by += m[j] * (s3 * ay - 3.0 * s5 * ar * ry);
+            bm += s3 * ar;
+        }
+        xbar[2 * j] += bx;
+        xbar[2 * j + 1] += by;
+        mbar[j] += bm;
+    }
+}
+
+void orc_force_vjp_fp64(const orc_params* p, uint32_t n, const float* mass, const float* pos,
+                        const float* abar, double* xbar, double* mbar) {
+    const size_t n2 = 2 * (size_t)n;
+    double* m = (double*)malloc(sizeof(double) * n);
+    double* x = (double*)malloc(sizeof(double) * n2);
+    double* ab = (double*)malloc(sizeof(double) * n2);
+    for (uint32_t i = 0; i < n; ++i) m[i] = mass[i];
+    for (size_t k = 0; k < n2; ++k) {
+        x[k] = pos[k];
+        ab[k] = abar[k];
+        xbar[k] = 0.0;
+    }
+    for (uint32_t i = 0; i < n; ++i) mbar[i] = 0.0;
+    ds_vjp(nthreads(p), n, p->grav_constant, (double)p->plummer_eps * (double)p->plummer_eps, m,
+           x, ab, xbar, mbar);
+    free(m); free(x); free(ab);
+}
+
+double orc_rollout_grad_fp64(const orc_params* p, uint32_t n, const float* mass, const float* pos,
+                             const float* vel, const float* target, uint32_t steps, double* gx,
+                             double* gv, double* gm) {
+    const int nt = nthreads(p);
+    const double G = p->grav_constant, dt = p->delta_time, h = 0.5 * dt;
+    const double e2 = (double)p->plummer_eps * (double)p->plummer_eps;
+    const size_t n2 = 2 * (size_t)n;
+    double* m = (double*)malloc(sizeof(double) * n);
+    double* xs = (double*)malloc(sizeof(double) * n2 * (steps + 1)); /* x_0 .. x_T */
+    double* v = (double*)malloc(sizeof(double) * n2);
+    double* a = (double*)malloc(sizeof(double) * n2);
+    double* ab = (double*)malloc(sizeof(double) * n2);
+    double* ap = (double*)calloc(n2, sizeof(double));
+    for (uint32_t i = 0; i < n; ++i) m[i] = mass[i];
+    for (size_t k = 0; k < n2; ++k) {
+        xs[k] = pos[k];
+        v[k] = vel[k];
+    }
+    ds_accel(nt, n, G, e2, m, xs, a);
+    for (uint32_t t = 0; t < steps; ++t) {
+        const double* x0 = xs + n2 * t;
+        double* x1 = xs + n2 * (t + 1);
+        for (size_t k = 0; k < n2; ++k) {
+            v[k] += h * a[k];
+            x1[k] = x0[k] + dt * v[k];
+        }
+        ds_accel(nt, n, G, e2, m, x1, a);
+        for (size_t k = 0; k < n2; ++k) v[k] += h * a[k];
+    }
+    const double* xT = xs + n2 * steps;
+    double L = 0.0;
+    for (size_t k = 0; k < n2; ++k) {
+        double d = xT[k] - target[k];
+        L += d * d / n;
+        gx[k] = 2.0 * d / n;
+        gv[k] = 0.0;
+    }
+    for (uint32_t i = 0; i < n; ++i) gm[i] = 0.0;
+    for (int64_t t = (int64_t)steps - 1; t >= 0; --t) {
+        for (size_t k = 0; k < n2; ++k) ab[k] = ap[k] + h * gv[k];
+        ds_vjp(nt, n, G, e2, m, xs + n2 * (t + 1), ab, gx, gm);
+        for (size_t k = 0; k < n2; ++k) {
+            gv[k] += dt * gx[k];
+            ap[k] = h * gv[k];
+        }
+    }
+    ds_vjp(nt, n, G, e2, m, xs, ap, gx, gm);
+    free(m); free(xs); free(v); free(a); free(ab); free(ap);
+    return L;
 }
 
 /* ------------------------------------------------------------------------ */

@@ -96,9 +96,9 @@ void orc_walk(const orc_params* p, uint32_t n, const uint32_t* ids, const float*
 void orc_quadrupoles(uint32_t n, const uint32_t* left, const uint32_t* right, const float* com,
                      const float* mass_node, float* quad);
 
-/* Extension: group walk.  Groups are runs of at most G = 32*bodies_per_lane
- * sorted slots cut from the maximal subtrees of at most 2G bodies; a group
- * opens a node unless L^2 < theta^2 d^2 (L = longest side of the node's
+/* Extension: group walk.  Groups are the maximal subtrees of at most
+ * G = 32*bodies_per_lane bodies (contiguous sorted slots); a group opens a
+ * node unless L^2 < theta^2 d^2 (L = longest side of the node's
  * box, d = distance between the group's box and the node's box); accepted
  * nodes act through monopole (+ quadrupole), leaves and opened nodes of
  * <= leaf_size bodies body by body.  acc[2*body]. */
@@ -115,6 +115,19 @@ void orc_walk_counts(const orc_params* p, uint32_t n, const uint32_t* ids, const
 /* FP64 direct sum for the listed bodies: acc_out[2*k] for body sample[k]. */
 void orc_direct_sum_fp64(const orc_params* p, uint32_t n, const float* mass, const float* pos,
                          uint32_t nsample, const uint32_t* sample, double* acc_out);
+
+/* Extension: FP64 direct-sum rollout of `steps` kick-drift-kick steps
+ * (Plummer softening) and its exact adjoint.  Returns
+ * L = (1/n) sum_i |x_T,i - target_i|^2 and writes dL/dx0 (gx[2n]),
+ * dL/dv0 (gv[2n]) and dL/dm (gm[n]). */
+double orc_rollout_grad_fp64(const orc_params* p, uint32_t n, const float* mass, const float* pos,
+                             const float* vel, const float* target, uint32_t steps, double* gx,
+                             double* gv, double* gm);
+
+/* Extension: FP64 direct-sum force VJP, xbar[2n] = (da/dx)^T abar and
+ * mbar[n] = (da/dm)^T abar (Plummer softening). */
+void orc_force_vjp_fp64(const orc_params* p, uint32_t n, const float* mass, const float* pos,
+                        const float* abar, double* xbar, double* mbar);
 
 /* Full state of a run: the buffers of simulation.ts:82-91 plus scratch. */
 typedef struct orc_state orc_state;

@@ -80,6 +80,9 @@ def load() -> ctypes.CDLL:
         "orc_get_state": (None, [_P, _P, _P]),
         "orc_get_tree": (None, [_P] + [_P] * 9),
         "orc_num_bodies": (ctypes.c_uint32, [_P]),
+        "orc_rollout_grad_fp64": (ctypes.c_double, [P, ctypes.c_uint32, _P, _P, _P, _P,
+                                                    ctypes.c_uint32, _P, _P, _P]),
+        "orc_force_vjp_fp64": (None, [P, ctypes.c_uint32, _P, _P, _P, _P, _P]),
         "orc_max_threads": (ctypes.c_int, []),
     }
     for name, (res, args) in sig.items():
@@ -194,6 +197,35 @@ def direct_sum_fp64(p: OrcParams, mass, pos, sample) -> np.ndarray:
     lib.orc_direct_sum_fp64(ctypes.byref(p), mass.size, _p(mass), _p(pos), sample.size,
                             _p(sample), _p(out))
     return out
+
+
+def rollout_grad_fp64(p: OrcParams, mass, pos, vel, target, steps: int):
+    """FP64 direct-sum KDK rollout and its exact adjoint: (L, dL/dx0, dL/dv0, dL/dm)."""
+    lib = load()
+    mass = f32(mass)
+    pos = f32(pos, (-1, 2))
+    vel = f32(vel, (-1, 2))
+    target = f32(target, (-1, 2))
+    n = mass.size
+    gx = np.zeros((n, 2), np.float64)
+    gv = np.zeros((n, 2), np.float64)
+    gm = np.zeros(n, np.float64)
+    L = lib.orc_rollout_grad_fp64(ctypes.byref(p), n, _p(mass), _p(pos), _p(vel), _p(target),
+                                  steps, _p(gx), _p(gv), _p(gm))
+    return float(L), gx, gv, gm
+
+
+def force_vjp_fp64(p: OrcParams, mass, pos, abar):
+    """FP64 direct-sum (da/dx)^T abar, (da/dm)^T abar."""
+    lib = load()
+    mass = f32(mass)
+    pos = f32(pos, (-1, 2))
+    abar = f32(abar, (-1, 2))
+    n = mass.size
+    xb = np.zeros((n, 2), np.float64)
+    mb = np.zeros(n, np.float64)
+    lib.orc_force_vjp_fp64(ctypes.byref(p), n, _p(mass), _p(pos), _p(abar), _p(xb), _p(mb))
+    return xb, mb
 
 
 REF_LIB = os.path.join(HERE, "_ref", "libref_wgsl.so")

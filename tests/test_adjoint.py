@@ -1,0 +1,128 @@
+"""Differentiable rollout: the adjoint tree walk and the reverse sweep.
+
+CPU: the FP64 direct-sum adjoint of the oracle against central finite
+differences of its own loss.
+GPU: the engine's force VJP against the FP64 direct-sum VJP; the rollout
+gradient (checkpoints every 20 steps, trees rebuilt on replay) against the
+FP64 direct-sum adjoint at N = 4,096 and against central finite differences
+(h = 1e-3, FP32) of the engine's own loss.
+"""
+import numpy as np
+import pytest
+
+THETA = 0.5
+EPS = 1e-3
+DT = 1e-4
+
+
+def adjoint_config(bh):
+    return bh.Config(bhTheta=THETA, deltaTime=DT, softening="plummer", plummerEps=EPS,
+                     mortonDomain="bbox", integrator="leapfrog-kdk", walk="group", leafSize=8)
+
+
+def test_fp64_adjoint_matches_finite_differences(orc):
+    rng = np.random.default_rng(0)
+    n = 40
+    pos = rng.normal(size=(n, 2)).astype(np.float32)
+    vel = (0.3 * rng.normal(size=(n, 2))).astype(np.float32)
+    mass = (rng.uniform(0.5, 1.5, n) / n).astype(np.float32)
+    tgt = (pos + 0.01 * rng.normal(size=(n, 2))).astype(np.float32)
+    p = orc.params(softening="plummer", plummer_eps=0.05, dt=1e-2)
+    _, gx, gv, gm = orc.rollout_grad_fp64(p, mass, pos, vel, tgt, 8)
+
+    def loss(m, x, v):
+        return orc.rollout_grad_fp64(p, m, x, v, tgt, 8)[0]
+
+    h = 1e-3
+    for which, arr, g in (("x", pos, gx), ("v", vel, gv), ("m", mass, gm)):
+        for idx in ((2, 0), (9, 1)) if which != "m" else ((2,), (9,)):
+            a1, a2 = arr.copy(), arr.copy()
+            a1[idx] += h
+            a2[idx] -= h
+            step = float(a1[idx]) - float(a2[idx])
+            args = {"x": lambda a: (mass, a, vel), "v": lambda a: (mass, pos, a),
+                    "m": lambda a: (a, pos, vel)}[which]
+            fd = (loss(*args(a1)) - loss(*args(a2))) / step
+            assert abs(fd - g[idx]) <= 1e-3 * abs(g[idx]) + 1e-9, (which, idx, fd, g[idx])
+
+
+def _target(bh, n, seed, steps):
+    """Target: the final positions of a rollout from velocities perturbed by N(0, 0.01^2)."""
+    mass, pos, vel, _ = bh.generate_scenario("uniform-disk-kepler", n, seed)
+    rng = np.random.default_rng(seed)
+    vel_t = (vel + 0.01 * rng.normal(size=vel.shape)).astype(np.float32)
+    sim = bh.Simulation(adjoint_config(bh))
+    sim.setNumBodies(n)
+    sim.upload(mass, pos, vel_t)
+    sim.step(steps)
+    _, tgt, _ = sim.download()
+    sim.close()
+    return mass, pos, vel, tgt
+
+
+@pytest.mark.gpu
+def test_force_vjp_matches_fp64_direct_sum(bh, orc):
+    n = 4096
+    mass, pos, vel, _ = bh.generate_scenario("uniform-disk-kepler", n, 3)
+    sim = bh.Simulation(adjoint_config(bh))
+    sim.setNumBodies(n)
+    sim.upload(mass, pos, vel)
+    abar = np.random.default_rng(1).normal(size=(n, 2)).astype(np.float32)
+    xb, mb = sim.force_vjp(abar)
+    xr, mr = orc.force_vjp_fp64(orc.params_from_config(sim.config), mass, pos, abar)
+    assert np.linalg.norm(xb - xr) <= 2e-2 * np.linalg.norm(xr)
+    assert np.linalg.norm(mb - mr) <= 2e-2 * np.linalg.norm(mr)
+    sim.close()
+
+
+@pytest.mark.gpu
+def test_rollout_gradient_matches_fp64_adjoint_4096(bh, orc):
+    n, steps = 4096, 200
+    mass, pos, vel, tgt = _target(bh, n, 5, steps)
+    sim = bh.Simulation(adjoint_config(bh))
+    sim.setNumBodies(n)
+    sim.upload(mass, pos, vel)
+    L, gx, gv, gm = sim.rollout_grad(steps, 20, tgt)
+    Lr, rx, rv, rm = orc.rollout_grad_fp64(orc.params_from_config(sim.config), mass, pos, vel, tgt,
+                                          steps)
+    assert abs(L - Lr) <= 1e-2 * Lr
+    for g, r in ((gx, rx), (gv, rv), (gm, rm)):
+        assert np.linalg.norm(g - r) <= 5e-2 * np.linalg.norm(r)
+        cos = float((g * r).sum() / (np.linalg.norm(g) * np.linalg.norm(r)))
+        assert cos > 0.995
+    # the handle is left at step T
+    _, p_end, _ = sim.download()
+    assert np.isfinite(p_end).all()
+    sim.close()
+
+
+@pytest.mark.gpu
+def test_rollout_gradient_matches_finite_differences(bh):
+    n, steps, h = 1024, 40, 1e-3
+    mass, pos, vel, tgt = _target(bh, n, 9, steps)
+    sim = bh.Simulation(adjoint_config(bh))
+    sim.setNumBodies(n)
+    sim.upload(mass, pos, vel)
+    _, gx, gv, gm = sim.rollout_grad(steps, 20, tgt)
+
+    def loss(m, x, v):
+        sim.upload(m, x, v)
+        sim.step(steps)
+        _, xT, _ = sim.download()
+        return float(((xT.astype(np.float64) - tgt) ** 2).sum() / n)
+
+    rng = np.random.default_rng(2)
+    for which in ("x", "v", "m"):
+        d = rng.normal(size=(n, 2) if which != "m" else n).astype(np.float32)
+        d /= np.linalg.norm(d)
+        if which == "m":
+            d = (d * mass / np.abs(mass).max()).astype(np.float32)
+        base = {"x": pos, "v": vel, "m": mass}[which]
+        plus, minus = base + h * d, base - h * d
+        args = {"x": lambda a: (mass, a, vel), "v": lambda a: (mass, pos, a),
+                "m": lambda a: (a, pos, vel)}[which]
+        fd = (loss(*args(plus)) - loss(*args(minus))) / (2 * h)
+        g = {"x": gx, "v": gv, "m": gm}[which]
+        ad = float((g.astype(np.float64) * d).sum())
+        assert abs(fd - ad) <= 5e-2 * abs(ad) + 1e-9, (which, fd, ad)
+    sim.close()

@@ -8,7 +8,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libbh_b200.so")
+# BH_B200_LIB overrides the library location (e.g. a build with other tunables).
+LIB_PATH = os.environ.get("BH_B200_LIB") or os.path.join(HERE, "libbh_b200.so")
 
 BH_OK = 0
 BH_ERR_INVALID_ARGUMENT = 1
@@ -103,6 +104,9 @@ SIGNATURES = {
     "bh_walk_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_uint64)]),
+    "bh_force_vjp": (ctypes.c_int, [_P, _P, _P, _P]),
+    "bh_rollout_grad": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, _P,
+                                       ctypes.POINTER(ctypes.c_float), _P, _P, _P]),
     "bh_build_hierarchy_static": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _P, ctypes.c_uint32,
                                                  _P, _P, _P, _P, ctypes.c_int32, _P]),
     "bh_last_error": (ctypes.c_char_p, [_P]),

@@ -44,6 +44,17 @@ struct bh_sim {
     bool profiling = false;
     uint32_t prof_max = 0, prof_used = 0;
     std::vector<cudaEvent_t> prof_ev;
+    // adjoint (bh_force_vjp / bh_rollout_grad), allocated on first use
+    struct Adjoint {
+        void* arena = nullptr;
+        uint32_t n = 0, nck = 0, seg = 0;
+        float* node_adj = nullptr;
+        float2 *xbar_slot = nullptr, *abar = nullptr, *xbar = nullptr, *vbar = nullptr,
+               *apend = nullptr, *target = nullptr, *ck_pos = nullptr, *ck_vel = nullptr,
+               *seg_pos = nullptr, *fin_pos = nullptr, *fin_vel = nullptr;
+        float *mbar_slot = nullptr, *mbar = nullptr;
+        double* loss = nullptr;
+    } adj;
     std::string err;
 };
 
@@ -136,8 +147,14 @@ static void destroy_graphs(bh_sim* s) {
     }
 }
 
+static void free_adjoint(bh_sim* s) {
+    if (s->adj.arena) cudaFree(s->adj.arena);
+    s->adj = bh_sim::Adjoint();
+}
+
 static void free_buffers(bh_sim* s) {
     destroy_graphs(s);
+    free_adjoint(s);
     if (s->arena) cudaFree(s->arena);
     s->arena = nullptr;
     s->arena_bytes = 0;
@@ -250,8 +267,7 @@ static bool needs_bbox(const bh_sim* s) {
 
 // Tree stages: scratch reset, bbox, Morton encode, sort, build + fill.
 template <class Mark>
-static void enqueue_tree(bh_sim* s, Mark mark) {
-    const DeviceBuffers& b = s->b;
+static void enqueue_tree_on(bh_sim* s, const DeviceBuffers& b, Mark mark) {
     cudaStream_t st = s->stream;
     cudaMemsetAsync(b.scratch, 0, sizeof(bh::StepScratch), st);
     cudaMemsetAsync(b.status, 0, sizeof(uint32_t) * (size_t)b.key_bytes * b.tiles * bh::kRadix, st);
@@ -263,6 +279,11 @@ static void enqueue_tree(bh_sim* s, Mark mark) {
     mark(3);
     bh::launch_build_fill(b, s->cfg.fp64_levels, st);
     mark(4);
+}
+
+template <class Mark>
+static void enqueue_tree(bh_sim* s, Mark mark) {
+    enqueue_tree_on(s, s->b, mark);
 }
 
 // One integration step (simulation.ts:394-420).
@@ -555,6 +576,169 @@ extern "C" int bh_compute_accelerations(bh_sim* s, float* acc_host) {
         BH_CUDA(s, cudaMemcpyAsync(acc_host, s->b.acc, 8 * (size_t)s->b.n, cudaMemcpyDeviceToHost, s->stream));
     BH_CUDA(s, cudaStreamSynchronize(s->stream));
     s->acc_valid = true;
+    return check_device_errors(s);
+}
+
+// ---- adjoint (extension) -----------------------------------------------------------
+
+namespace bh {
+void launch_force_vjp(const DeviceBuffers& b, const WalkParams& p, const float2* abar,
+                      float* node_adj, float2* xbar_slot, float* mbar_slot, float2* xbar,
+                      float* mbar, cudaStream_t s);
+void launch_adj_init(const float2* pos, const float2* target, uint32_t n, float2* xbar,
+                     float2* vbar, float* mbar, float2* apend, double* loss, cudaStream_t s);
+void launch_adj_pre(const float2* apend, const float2* vbar, float h, uint32_t n, float2* abar,
+                    cudaStream_t s);
+void launch_adj_post(const float2* xbar, float2* vbar, float2* apend, float dt, float h, uint32_t n,
+                     cudaStream_t s);
+}  // namespace bh
+
+static int adjoint_supported(bh_sim* s) {
+    if (s->cfg.walk_mode != BH_WALK_GROUP || s->cfg.softening != BH_SOFTENING_PLUMMER)
+        return fail(s, BH_ERR_NOT_SUPPORTED,
+                    "the adjoint needs the group walk and Plummer softening");
+    return BH_OK;
+}
+
+static int ensure_adjoint(bh_sim* s, uint32_t nck, uint32_t seg) {
+    const uint32_t n = s->b.n;
+    bh_sim::Adjoint& a = s->adj;
+    if (a.arena && a.n == n && a.nck >= nck && a.seg >= seg) return BH_OK;
+    free_adjoint(s);
+    const size_t nb = n ? n : 1, ni = n > 1 ? n - 1 : 1;
+    Carver c;
+    size_t o_na = c.take<float>(6 * ni), o_xs = c.take<float2>(nb), o_ms = c.take<float>(nb);
+    size_t o_ab = c.take<float2>(nb), o_xb = c.take<float2>(nb), o_vb = c.take<float2>(nb);
+    size_t o_mb = c.take<float>(nb), o_ap = c.take<float2>(nb), o_tg = c.take<float2>(nb);
+    size_t o_cp = c.take<float2>(nb * nck), o_cv = c.take<float2>(nb * nck);
+    size_t o_sp = c.take<float2>(nb * (seg + 1)), o_fp = c.take<float2>(nb), o_fv = c.take<float2>(nb);
+    size_t o_ls = c.take<double>(1);
+    void* arena = nullptr;
+    cudaError_t e = cudaMalloc(&arena, c.off);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(s, e, "cudaMalloc(adjoint buffers)");
+    }
+    char* p = (char*)arena;
+    a.arena = arena;
+    a.n = n;
+    a.nck = nck;
+    a.seg = seg;
+    a.node_adj = (float*)(p + o_na);
+    a.xbar_slot = (float2*)(p + o_xs);
+    a.mbar_slot = (float*)(p + o_ms);
+    a.abar = (float2*)(p + o_ab);
+    a.xbar = (float2*)(p + o_xb);
+    a.vbar = (float2*)(p + o_vb);
+    a.mbar = (float*)(p + o_mb);
+    a.apend = (float2*)(p + o_ap);
+    a.target = (float2*)(p + o_tg);
+    a.ck_pos = (float2*)(p + o_cp);
+    a.ck_vel = (float2*)(p + o_cv);
+    a.seg_pos = (float2*)(p + o_sp);
+    a.fin_pos = (float2*)(p + o_fp);
+    a.fin_vel = (float2*)(p + o_fv);
+    a.loss = (double*)(p + o_ls);
+    return BH_OK;
+}
+
+// (xbar, mbar) += J^T abar for the force at positions `at` (tree rebuilt there).
+static void enqueue_force_vjp(bh_sim* s, const float2* at, const float2* abar) {
+    DeviceBuffers bb = s->b;
+    bb.pos = const_cast<float2*>(at);
+    enqueue_tree_on(s, bb, [](int) {});
+    bh::launch_force_vjp(bb, walk_params(s, bh::kWalkForces), abar, s->adj.node_adj,
+                         s->adj.xbar_slot, s->adj.mbar_slot, s->adj.xbar, s->adj.mbar, s->stream);
+}
+
+extern "C" int bh_force_vjp(bh_sim* s, const float* abar, float* xbar, float* mbar) {
+    BH_HANDLE(s);
+    int rc = adjoint_supported(s);
+    if (rc != BH_OK) return rc;
+    const uint32_t n = s->b.n;
+    if (n == 0) return BH_OK;
+    if (!abar) return fail(s, BH_ERR_INVALID_ARGUMENT, "null abar");
+    if ((rc = ensure_adjoint(s, 1, 1)) != BH_OK) return rc;
+    bh_sim::Adjoint& a = s->adj;
+    BH_CUDA(s, cudaMemcpyAsync(a.abar, abar, 8 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    BH_CUDA(s, cudaMemsetAsync(a.xbar, 0, 8 * (size_t)n, s->stream));
+    BH_CUDA(s, cudaMemsetAsync(a.mbar, 0, 4 * (size_t)n, s->stream));
+    enqueue_force_vjp(s, s->b.pos, a.abar);
+    BH_CUDA(s, cudaGetLastError());
+    if (xbar) BH_CUDA(s, cudaMemcpyAsync(xbar, a.xbar, 8 * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
+    if (mbar) BH_CUDA(s, cudaMemcpyAsync(mbar, a.mbar, 4 * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
+    BH_CUDA(s, cudaStreamSynchronize(s->stream));
+    return check_device_errors(s);
+}
+
+extern "C" int bh_rollout_grad(bh_sim* s, uint32_t steps, uint32_t checkpoint_every,
+                               const float* target_pos, float* loss, float* grad_pos,
+                               float* grad_vel, float* grad_mass) {
+    BH_HANDLE(s);
+    int rc = adjoint_supported(s);
+    if (rc != BH_OK) return rc;
+    if (s->cfg.integrator != BH_INTEGRATOR_LEAPFROG_KDK)
+        return fail(s, BH_ERR_NOT_SUPPORTED, "the rollout gradient needs the leapfrog integrator");
+    if (steps == 0 || checkpoint_every == 0 || !target_pos)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "steps, checkpoint_every and target_pos are required");
+    const uint32_t n = s->b.n;
+    if (n == 0) return BH_OK;
+    const uint32_t K = checkpoint_every < steps ? checkpoint_every : steps;
+    const uint32_t nck = (steps + K - 1) / K;  // checkpoints at 0, K, 2K, ... < steps
+    if ((rc = ensure_adjoint(s, nck, K)) != BH_OK) return rc;
+    bh_sim::Adjoint& a = s->adj;
+    cudaStream_t st = s->stream;
+    const size_t vb = 8 * (size_t)n;
+    const float dt = s->cfg.delta_time, h = 0.5f * dt;
+    BH_CUDA(s, cudaMemcpyAsync(a.target, target_pos, vb, cudaMemcpyHostToDevice, st));
+    // Forward: T steps, saving (x, v) at every checkpoint.
+    for (uint32_t k = 0; k < steps; ++k) {
+        if (k % K == 0) {
+            BH_CUDA(s, cudaMemcpyAsync(a.ck_pos + (size_t)(k / K) * n, s->b.pos, vb, cudaMemcpyDeviceToDevice, st));
+            BH_CUDA(s, cudaMemcpyAsync(a.ck_vel + (size_t)(k / K) * n, s->b.vel, vb, cudaMemcpyDeviceToDevice, st));
+        }
+        if ((rc = step_once(s)) != BH_OK) return rc;
+    }
+    BH_CUDA(s, cudaMemcpyAsync(a.fin_pos, s->b.pos, vb, cudaMemcpyDeviceToDevice, st));
+    BH_CUDA(s, cudaMemcpyAsync(a.fin_vel, s->b.vel, vb, cudaMemcpyDeviceToDevice, st));
+    // dL/dx_T for L = (1/n) sum_i |x_T,i - target_i|^2
+    bh::launch_adj_init(s->b.pos, a.target, n, a.xbar, a.vbar, a.mbar, a.apend, a.loss, st);
+    // Reverse sweep, one checkpoint segment at a time (replay rebuilds the trees).
+    for (int64_t seg = (int64_t)nck - 1; seg >= 0; --seg) {
+        const uint32_t c = (uint32_t)seg * K, e = (c + K < steps) ? c + K : steps;
+        BH_CUDA(s, cudaMemcpyAsync(s->b.pos, a.ck_pos + (size_t)seg * n, vb, cudaMemcpyDeviceToDevice, st));
+        BH_CUDA(s, cudaMemcpyAsync(s->b.vel, a.ck_vel + (size_t)seg * n, vb, cudaMemcpyDeviceToDevice, st));
+        s->acc_valid = false;
+        BH_CUDA(s, cudaMemcpyAsync(a.seg_pos, s->b.pos, vb, cudaMemcpyDeviceToDevice, st));
+        for (uint32_t k = c; k < e; ++k) {
+            if ((rc = step_once(s)) != BH_OK) return rc;
+            BH_CUDA(s, cudaMemcpyAsync(a.seg_pos + (size_t)(k + 1 - c) * n, s->b.pos, vb,
+                                       cudaMemcpyDeviceToDevice, st));
+        }
+        for (int64_t k = (int64_t)e - 1; k >= (int64_t)c; --k) {
+            // closing kick of step k (force at x_{k+1}) plus the pending opening
+            // kick of step k+1 at the same point
+            bh::launch_adj_pre(a.apend, a.vbar, h, n, a.abar, st);
+            enqueue_force_vjp(s, a.seg_pos + (size_t)(k + 1 - c) * n, a.abar);
+            // drift, then the opening kick of step k (force at x_k, pending)
+            bh::launch_adj_post(a.xbar, a.vbar, a.apend, dt, h, n, st);
+        }
+    }
+    // the opening kick of step 0 acts at x_0
+    bh::launch_adj_pre(a.apend, a.vbar, 0.0f, n, a.abar, st);
+    enqueue_force_vjp(s, a.ck_pos, a.abar);
+    BH_CUDA(s, cudaGetLastError());
+    double L = 0.0;
+    BH_CUDA(s, cudaMemcpyAsync(&L, a.loss, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (grad_pos) BH_CUDA(s, cudaMemcpyAsync(grad_pos, a.xbar, vb, cudaMemcpyDeviceToHost, st));
+    if (grad_vel) BH_CUDA(s, cudaMemcpyAsync(grad_vel, a.vbar, vb, cudaMemcpyDeviceToHost, st));
+    if (grad_mass) BH_CUDA(s, cudaMemcpyAsync(grad_mass, a.mbar, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
+    // leave the handle at step T
+    BH_CUDA(s, cudaMemcpyAsync(s->b.pos, a.fin_pos, vb, cudaMemcpyDeviceToDevice, st));
+    BH_CUDA(s, cudaMemcpyAsync(s->b.vel, a.fin_vel, vb, cudaMemcpyDeviceToDevice, st));
+    s->acc_valid = false;
+    BH_CUDA(s, cudaStreamSynchronize(st));
+    if (loss) *loss = (float)L;
     return check_device_errors(s);
 }
 

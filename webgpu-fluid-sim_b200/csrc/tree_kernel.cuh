@@ -187,25 +187,14 @@ build_fill_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ ids,
             gnode[pidx] = g;
         }
         if (groups) {
-            // Walk groups: the maximal subtrees of <= 2 gmax bodies, cut into
-            // runs of gmax slots (a child is such a subtree when its parent is
-            // bigger; the whole tree is one when n <= 2 gmax).
-            const uint32_t gsub = 2u * gmax;
-            auto emit = [&](uint32_t f, uint32_t c) {
-                if (c <= gmax) {
-                    groups[atomicAdd(group_count, 1u)] = make_uint2(f, c);
-                } else {
-                    const uint32_t at = atomicAdd(group_count, 2u);
-                    groups[at] = make_uint2(f, gmax);
-                    groups[at + 1] = make_uint2(f + gmax, c - gmax);
-                }
-            };
-            if (cnt > gsub) {
+            // Walk groups: maximal subtrees of <= gmax bodies.  A child is one
+            // when its parent is too big; the whole tree is one when n <= gmax.
+            if (cnt > gmax) {
                 const uint32_t lcnt = gamma - pl + 1, rcnt = pr - gamma;
-                if (lcnt <= gsub) emit(pl, lcnt);
-                if (rcnt <= gsub) emit(gamma + 1, rcnt);
+                if (lcnt <= gmax) groups[atomicAdd(group_count, 1u)] = make_uint2(pl, lcnt);
+                if (rcnt <= gmax) groups[atomicAdd(group_count, 1u)] = make_uint2(gamma + 1, rcnt);
             } else if (pidx == 0) {
-                emit(0u, n);
+                groups[atomicAdd(group_count, 1u)] = make_uint2(0u, n);
             }
         }
         node4[pidx] = make_float4(ncx, ncy, tm, len);

@@ -6,12 +6,12 @@
 // walk has a median relative force error of order 1e-2 at theta = 0.5 in 2D;
 // this walk reaches <= 1e-3 at the same theta.
 //
-// One warp owns a group: a run of at most G = 32 x BPL sorted slots cut from
-// a maximal subtree of at most 2G bodies, so its bodies lie inside one Morton
-// cell (the build kernel lists the groups).  Fixed runs of G slots over the
-// whole order would not do: a run that straddles a jump of the Z curve has a
-// box spanning far-apart regions and opens nearly every node; whole maximal
-// G-body subtrees would do but leave about 30% of the lanes idle.  The group
+// One warp owns a group: a maximal subtree of at most G = 32 x BPL bodies, so
+// its bodies are contiguous sorted slots inside one Morton cell (the build
+// kernel lists the groups).  Fixed runs of G slots would not do: a run that
+// straddles a jump of the Z curve has a box spanning far-apart regions and
+// opens nearly every node.  (Cutting maximal 2G-body subtrees into G-slot
+// runs fills more lanes but opens more nodes; measured slower.)  The group
 // opens a node unless
 //     L^2 < theta^2 d^2,  L = longest side of the node's box,
 //     d = distance between the group's box and the node's box,
@@ -95,8 +95,12 @@ __device__ __forceinline__ f2x ld_pair(const float4& v, int half) {
     return reinterpret_cast<const f2x*>(&v)[half];
 }
 
+#ifndef BH_WALK_MIN_BLOCKS
+#define BH_WALK_MIN_BLOCKS 8  // resident blocks per SM the register budget is sized for
+#endif
+
 template <int BPL, int MP, bool PLUMMER>
-__global__ void __launch_bounds__(kGroupWarps * 32, 8)
+__global__ void __launch_bounds__(kGroupWarps * 32, BH_WALK_MIN_BLOCKS)
 walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ node4,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ ids,
                   float2* __restrict__ pos, float2* __restrict__ vel, float2* __restrict__ acc,
@@ -186,8 +190,8 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
                             const f2x nqry = fma2(NQXY, rx, mul2(NQYY, ry));  // -(Q'r)_y
                             const f2x nrqr = fma2(rx, nqrx, mul2(ry, nqry)); // -r.Q'r
                             const f2x inv5 = mul2(inv3, inv2);
-                            // f = (m + 5/2 r.Q'r / |r|^2) / |r|^3
-                            const f2x f = mul2(inv3, fma2(nrqr, mul2(M25, inv2), M));
+                            // f = m / |r|^3 + 5/2 r.Q'r / |r|^7
+                            const f2x f = fma2(mul2(nrqr, M25), mul2(inv5, inv2), mul2(M, inv3));
                             AX[q] = fma2(nqrx, inv5, fma2(f, rx, AX[q]));
                             AY[q] = fma2(nqry, inv5, fma2(f, ry, AY[q]));
                         } else {

@@ -203,6 +203,28 @@ class Simulation:
         self._check(self._lib.bh_profile_end(self._h, ms, ctypes.byref(cnt)))
         return {k: float(ms[i]) for i, k in enumerate(_lib.BH_STAGE_NAMES)}, int(cnt.value)
 
+    def force_vjp(self, abar) -> tuple[np.ndarray, np.ndarray]:
+        """(da/dx)^T abar and (da/dm)^T abar at the current positions."""
+        n = self.getNumBodies()
+        ab = _as_host_f32(abar, 2 * n)
+        xbar = np.empty((n, 2), np.float32)
+        mbar = np.empty(n, np.float32)
+        self._check(self._lib.bh_force_vjp(self._h, _ptr(ab), _ptr(xbar), _ptr(mbar)))
+        return xbar, mbar
+
+    def rollout_grad(self, steps: int, checkpoint_every: int, target_pos):
+        """Loss (1/n) sum |x_T - target|^2 after `steps` steps and its gradient
+        w.r.t. the initial positions, velocities and masses."""
+        n = self.getNumBodies()
+        tg = _as_host_f32(target_pos, 2 * n)
+        loss = ctypes.c_float()
+        gx = np.empty((n, 2), np.float32)
+        gv = np.empty((n, 2), np.float32)
+        gm = np.empty(n, np.float32)
+        self._check(self._lib.bh_rollout_grad(self._h, int(steps), int(checkpoint_every), _ptr(tg),
+                                              ctypes.byref(loss), _ptr(gx), _ptr(gv), _ptr(gm)))
+        return float(loss.value), gx, gv, gm
+
     def walk_stats(self) -> tuple[int, int, int]:
         """(node visits, multipole interactions, body interactions) at the current positions."""
         v = ctypes.c_uint64()
