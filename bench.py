@@ -55,7 +55,78 @@ def parse():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true")
     return ap.parse_args()
+
+
+def adjoint_cost(pkg, device: int, n: int = 65536, steps: int = 200, every: int = 20) -> dict:
+    """Differentiable-rollout cost: N = 65,536 uniform disk, theta 0.5, eps 1e-3,
+    dt 1e-4, T = 200 leapfrog steps, checkpoints every 20; the target is the
+    rollout from velocities perturbed by N(0, 0.01^2).  Reports adjoint time /
+    forward-rollout time and the speed-up over a central finite-difference
+    gradient (2 rollouts per parameter, 5 parameters per body)."""
+    cfg = pkg.Config(bhTheta=0.5, deltaTime=1e-4, softening="plummer", plummerEps=1e-3,
+                     mortonDomain="bbox", integrator="leapfrog-kdk", walk="group", leafSize=4)
+    mass, pos, vel, _ = pkg.generate_scenario("uniform-disk-kepler", n, 3)
+    sim = pkg.Simulation(cfg, device=device)
+    sim.setNumBodies(n)
+    rng = np.random.default_rng(0)
+    sim.upload(mass, pos, (vel + 0.01 * rng.normal(size=vel.shape)).astype(np.float32))
+    sim.step(steps)
+    _, tgt, _ = sim.download()
+    best_f, best_a = 1e30, 1e30
+    for _ in range(3):
+        sim.upload(mass, pos, vel)
+        sim.sync()
+        t0 = time.perf_counter()
+        sim.step(steps)
+        sim.sync()
+        best_f = min(best_f, time.perf_counter() - t0)
+        sim.upload(mass, pos, vel)
+        sim.sync()
+        t0 = time.perf_counter()
+        loss, _, _, _ = sim.rollout_grad(steps, every, tgt)
+        best_a = min(best_a, time.perf_counter() - t0)
+    sim.close()
+    fd = best_f * 2 * 5 * n
+    return {"bodies": n, "steps": steps, "checkpoint_every": every, "forward_s": best_f,
+            "adjoint_s": best_a, "adjoint_over_forward": best_a / best_f,
+            "fd_gradient_s_estimate": fd, "speedup_vs_fd": fd / best_a, "loss": loss,
+            "timing": "host wall clock around synchronised calls, best of 3"}
+
+
+def secondary_16m(pkg, device: int, steps: int = 5) -> dict:
+    """The 16.8M-body Gaussian-mixture point of the metric (64-bit keys)."""
+    import torch
+    wl = pkg.WORKLOADS["gaussian-mixture-16m"]
+    sim = pkg.Simulation(wl["config"], device=device)
+    sim.setNumBodies(wl["n"])
+    sim.setScenario(wl["scenario"], 1)
+    tune = sim.autotune(2)
+    for _ in range(3):
+        sim.step(1)
+    sim.sync()
+    ext = torch.cuda.ExternalStream(sim.getBuffers().stream, device=torch.device("cuda", device))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    sim.profile_begin(steps)
+    e0.record(ext)
+    sim.step(steps)
+    e1.record(ext)
+    sim.sync()
+    stage_ms, rec = sim.profile_end()
+    ms = e0.elapsed_time(e1) / steps
+    mass, pos, _ = sim.download()
+    acc = sim.computeAccelerations()
+    med, p99, ns = force_error_vs_fp64(acc, mass, pos, wl["config"], nsample=64)
+    sim.close()
+    return {"workload": "gaussian-mixture-16m", "bodies": wl["n"], "value": wl["n"] / (ms / 1e3),
+            "unit": "body-steps/s", "ms_per_step": ms,
+            "stages_ms": {k: v / max(rec, 1) for k, v in stage_ms.items()},
+            "force_error_vs_fp64": {"median": med, "p99": p99, "sample": ns}, "autotune": tune,
+            "l2": "working set 3 GB > L2"}
 
 
 # ---------------------------------------------------------------- helpers
@@ -243,6 +314,8 @@ def run_own(args):
     sim = pkg.Simulation(cfg, device=local)
     sim.setNumBodies(n)
     sim.setScenario(wl["scenario"], 1 + rank)
+    tune = None if args.no_autotune else sim.autotune(3)
+    cfg = sim.config
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     ext = torch.cuda.ExternalStream(sim.getBuffers().stream, device=dev)
@@ -363,6 +436,9 @@ def run_own(args):
             "config": {"workload": args.workload, "bodies": n, "theta": cfg.bhTheta,
                        "softening": f"plummer {cfg.plummerEps}", "dt": cfg.deltaTime,
                        "integrator": cfg.integrator, "morton_bits": cfg.mortonBits,
+                       "walk": f"{cfg.walk}, multipole order {cfg.multipole}",
+                       "bodies_per_lane": cfg.bodiesPerLane, "leaf_size": cfg.leafSize,
+                       "autotuned": tune is not None,
                        "parallelism": f"replicas{world}" if world > 1 else "single",
                        "l2": "flushed between timed steps (256 MB write, outside the events)"},
             "roofline": roofline,
@@ -376,8 +452,13 @@ def run_own(args):
             "clocks": clk,
             "wall_s_timed_region": wall,
         }
-        print(json.dumps(out))
     sim.close()
+    if rank == 0:
+        if not args.no_secondary and args.workload != "gaussian-mixture-16m":
+            out["secondary"] = secondary_16m(pkg, local)
+        if not args.no_adjoint:
+            out["adjoint"] = adjoint_cost(pkg, local)
+        print(json.dumps(out))
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

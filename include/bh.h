@@ -181,6 +181,23 @@ int bh_generate_scenario(const char* name, uint32_t n, uint64_t seed, float grav
 int bh_profile_begin(bh_sim* sim, uint32_t max_steps);
 int bh_profile_end(bh_sim* sim, double* stage_ms, uint32_t* steps_recorded);
 
+/* ---- autotuner (extension; no reference counterpart) -------------------- */
+typedef struct bh_tune_result {
+    int32_t bodies_per_lane; /* chosen walk group shape: 32 x this many bodies per warp */
+    int32_t leaf_size;       /* chosen bucket size */
+    float walk_ms;           /* its average walk time */
+    int32_t candidates;      /* candidates timed */
+} bh_tune_result;
+
+/* Time the group walk (on force evaluations at the current positions, which
+ * do not advance the state) for bodies_per_lane in {1, 2, 4} x leaf_size in
+ * {2, 4, 8}, `trials` launches each after one warm-up, and keep the fastest
+ * in the handle's configuration.  Group walk only. */
+int bh_autotune(bh_sim* sim, uint32_t trials, bh_tune_result* out);
+
+/* The handle's current configuration (after bh_autotune, for instance). */
+int bh_get_config(bh_sim* sim, bh_config* out);
+
 /* Kernels one step launches (for launch accounting). */
 int bh_kernels_per_step(bh_sim* sim, uint32_t* out);
 

@@ -257,6 +257,30 @@ def test_walk_stats_counts(bh):
     sim2.close()
 
 
+def test_autotune_picks_a_valid_config_and_stays_accurate(bh, orc):
+    import ctypes
+    sim = make_sim(bh, 100000, "colliding-disks", seed=4, **GROUP)
+    mass, pos, vel = sim.download()
+    r = sim.autotune(2)
+    assert r["candidates"] == 9
+    assert r["bodiesPerLane"] in (1, 2, 4) and r["leafSize"] in (2, 4, 8) and r["walk_ms"] > 0
+    c = bh._lib.bh_config() if hasattr(bh, "_lib") else None
+    lib = bh.load()
+    from importlib import import_module
+    cfg = import_module("webgpu-fluid-sim_b200._lib").bh_config()
+    assert lib.bh_get_config(sim._h, ctypes.byref(cfg)) == 0
+    assert (cfg.bodies_per_lane, cfg.leaf_size) == (r["bodiesPerLane"], r["leafSize"])
+    acc = sim.computeAccelerations()
+    sample = np.random.default_rng(1).choice(100000, 200, replace=False)
+    ref = orc.direct_sum_fp64(orc.params_from_config(sim.config), mass, pos, sample)
+    err = np.linalg.norm(acc[sample] - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    assert np.median(err) <= 1e-3
+    # the state did not move
+    _, p2, _ = sim.download()
+    assert np.array_equal(p2, pos)
+    sim.close()
+
+
 def test_unknown_scenario_raises(bh):
     sim = bh.Simulation()
     with pytest.raises(bh.BhError, match="Unknown scenario: nope"):

@@ -58,6 +58,15 @@ BH_WALK_EXACT = 0
 BH_WALK_GROUP = 1
 
 
+class bh_tune_result(ctypes.Structure):
+    _fields_ = [
+        ("bodies_per_lane", ctypes.c_int32),
+        ("leaf_size", ctypes.c_int32),
+        ("walk_ms", ctypes.c_float),
+        ("candidates", ctypes.c_int32),
+    ]
+
+
 class bh_buffers(ctypes.Structure):
     _fields_ = [
         ("mass", ctypes.c_void_p),
@@ -104,6 +113,8 @@ SIGNATURES = {
     "bh_walk_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_uint64)]),
+    "bh_autotune": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(bh_tune_result)]),
+    "bh_get_config": (ctypes.c_int, [_P, ctypes.POINTER(bh_config)]),
     "bh_force_vjp": (ctypes.c_int, [_P, _P, _P, _P]),
     "bh_rollout_grad": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, _P,
                                        ctypes.POINTER(ctypes.c_float), _P, _P, _P]),

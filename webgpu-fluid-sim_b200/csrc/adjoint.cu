@@ -36,8 +36,9 @@ constexpr int kVjpSlots = 32 + 32 * kGroupMaxLeaf;
 
 struct VjpSmem {
     uint32_t stack[kVjpStack];
-    uint32_t node[kGroupList];
+    float4 nd[kGroupList][2];  // {cx, cy, m, node index bits}, {Q'xx, Q'xy, Q'yy, 0}
     uint32_t slot[kVjpSlots];
+    float4 body[32];           // staged leaf records {x, y, m, slot bits}
 };
 
 __device__ __forceinline__ float warp_sum(float v) {
@@ -100,14 +101,10 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
 
         auto eval_nodes = [&](int cnt) {
             for (int j = 0; j < cnt; ++j) {
-                const uint32_t v = S.node[j];
-                const float4 mom = __ldg(&gnode[v].mom);
-                float qxx = 0.f, qxy = 0.f, qyy = 0.f;
-                if (MP >= 2) {
-                    const float4 sq = __ldg(&gnode[v].quad);
-                    const float tr = sq.x + sq.z;
-                    qxx = 3.0f * sq.x - tr; qxy = 3.0f * sq.y; qyy = 3.0f * sq.z - tr;
-                }
+                const float4 mom = S.nd[j][0];
+                const uint32_t v = __float_as_uint(mom.w);
+                const float4 q4 = S.nd[j][1];
+                const float qxx = q4.x, qxy = q4.y, qyy = q4.z;
                 float cbx = 0.f, cby = 0.f, mb = 0.f, gxx = 0.f, gxy = 0.f, gyy = 0.f;
 #pragma unroll
                 for (int k = 0; k < BPL; ++k) {
@@ -160,8 +157,18 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
         };
         auto eval_bodies = [&](int cnt) {
             for (int j = 0; j < cnt; ++j) {
-                const uint32_t sj = S.slot[j];
-                const float4 o = __ldg(&node4[nm1 + sj]);
+                if ((j & 31) == 0) {  // stage the next 32 leaf records in parallel
+                    __syncwarp();
+                    if (j + lane < cnt) {
+                        const uint32_t sl = S.slot[j + lane];
+                        float4 r = __ldg(&node4[nm1 + sl]);
+                        r.w = __uint_as_float(sl);
+                        S.body[lane] = r;
+                    }
+                    __syncwarp();
+                }
+                const float4 o = S.body[j & 31];
+                const uint32_t sj = __float_as_uint(o.w);
                 float cbx = 0.f, cby = 0.f, mb = 0.f;
 #pragma unroll
                 for (int k = 0; k < BPL; ++k) {
@@ -205,6 +212,7 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
             __syncwarp();
             bool emit_node = false, emit_range = false, push = false;
             uint32_t r0 = 0, r1 = 0;
+            float4 mom = make_float4(0.f, 0.f, 0.f, 0.f), sq = mom;
             if (has) {
                 if (v >= nm1) {
                     emit_range = true;
@@ -213,6 +221,8 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
                 } else {
                     const float4 box = __ldg(&gnode[v].box);
                     const uint4 lk = __ldg(&gnode[v].link);
+                    mom = __ldg(&gnode[v].mom);
+                    if (MP >= 2) sq = __ldg(&gnode[v].quad);
                     const float dx = fmaxf(0.0f, fmaxf(__fsub_rn(box.x, ghix), __fsub_rn(glox, box.z)));
                     const float dy = fmaxf(0.0f, fmaxf(__fsub_rn(box.y, ghiy), __fsub_rn(gloy, box.w)));
                     const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
@@ -231,7 +241,12 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
                 }
             }
             const unsigned mn = __ballot_sync(FULL, emit_node);
-            if (emit_node) S.node[nn + __popc(mn & lt)] = v;
+            if (emit_node) {
+                const int p = nn + __popc(mn & lt);
+                S.nd[p][0] = make_float4(mom.x, mom.y, mom.z, __uint_as_float(v));
+                const float tr = sq.x + sq.z;  // Q' = 3S - tr(S) I
+                S.nd[p][1] = make_float4(3.0f * sq.x - tr, 3.0f * sq.y, 3.0f * sq.z - tr, 0.0f);
+            }
             nn += __popc(mn);
             {
                 const uint32_t c = emit_range ? r1 : 0u;

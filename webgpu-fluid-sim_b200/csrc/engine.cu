@@ -856,6 +856,74 @@ extern "C" int bh_profile_end(bh_sim* s, double* stage_ms, uint32_t* steps_recor
     return check_device_errors(s);
 }
 
+// ---- autotuner (extension) -----------------------------------------------------------
+// Times the group walk on force evaluations at the current positions (which
+// do not advance the state) for every (bodies per lane, leaf size) candidate
+// and keeps the fastest.  The walk's result depends on both (group boxes and
+// bucket sizes change the interaction lists), so every candidate is a valid
+// configuration with its own accuracy; all stay far inside the group walk's
+// error budget at a given theta.
+extern "C" int bh_autotune(bh_sim* s, uint32_t trials, bh_tune_result* out) {
+    BH_HANDLE(s);
+    if (s->cfg.walk_mode != BH_WALK_GROUP)
+        return fail(s, BH_ERR_NOT_SUPPORTED, "the autotuner tunes the group walk");
+    if (trials == 0) trials = 3;
+    static const int kBpl[] = {1, 2, 4};
+    static const int kLeaf[] = {2, 4, 8};
+    bh_tune_result best{};
+    best.walk_ms = 1e30f;
+    cudaEvent_t e0, e1;
+    BH_CUDA(s, cudaEventCreate(&e0));
+    BH_CUDA(s, cudaEventCreate(&e1));
+    int count = 0;
+    const bh_config saved = s->cfg;
+    for (int bpl : kBpl) {
+        for (int leaf : kLeaf) {
+            s->cfg.bodies_per_lane = bpl;
+            s->cfg.leaf_size = leaf;
+            s->b.group_max = 32u * (uint32_t)bpl;
+            if (s->b.n == 0) break;
+            float total = 0.f;
+            for (uint32_t t = 0; t <= trials; ++t) {  // trial 0 warms up
+                enqueue_tree(s, [](int) {});
+                cudaEventRecord(e0, s->stream);
+                launch_walk_any(s, walk_params(s, bh::kWalkForces));
+                cudaEventRecord(e1, s->stream);
+                BH_CUDA(s, cudaEventSynchronize(e1));
+                float ms = 0.f;
+                BH_CUDA(s, cudaEventElapsedTime(&ms, e0, e1));
+                if (t > 0) total += ms;
+            }
+            const float avg = total / (float)trials;
+            ++count;
+            if (avg < best.walk_ms) {
+                best.walk_ms = avg;
+                best.bodies_per_lane = bpl;
+                best.leaf_size = leaf;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->cfg = saved;
+    if (count > 0) {
+        s->cfg.bodies_per_lane = best.bodies_per_lane;
+        s->cfg.leaf_size = best.leaf_size;
+    }
+    s->b.group_max = 32u * (uint32_t)(s->cfg.bodies_per_lane > 0 ? s->cfg.bodies_per_lane : 2);
+    destroy_graphs(s);  // captured steps carry the old walk parameters
+    s->acc_valid = false;
+    best.candidates = count;
+    if (out) *out = best;
+    return check_device_errors(s);
+}
+
+extern "C" int bh_get_config(bh_sim* s, bh_config* out) {
+    if (!s || !out) return fail(s, BH_ERR_INVALID_ARGUMENT, "null argument");
+    *out = s->cfg;
+    return BH_OK;
+}
+
 extern "C" int bh_kernels_per_step(bh_sim* s, uint32_t* out) {
     if (!s || !out) return fail(s, BH_ERR_INVALID_ARGUMENT, "null argument");
     uint32_t k = 0;

@@ -96,7 +96,7 @@ __device__ __forceinline__ f2x ld_pair(const float4& v, int half) {
 }
 
 #ifndef BH_WALK_MIN_BLOCKS
-#define BH_WALK_MIN_BLOCKS 8  // resident blocks per SM the register budget is sized for
+#define BH_WALK_MIN_BLOCKS 6  // resident blocks per SM the register budget is sized for (measured best)
 #endif
 
 template <int BPL, int MP, bool PLUMMER>
