@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     return ap.parse_args()
 
 
@@ -127,6 +128,96 @@ def secondary_16m(pkg, device: int, steps: int = 5) -> dict:
             "stages_ms": {k: v / max(rec, 1) for k, v in stage_ms.items()},
             "force_error_vs_fp64": {"median": med, "p99": p99, "sample": ns}, "autotune": tune,
             "l2": "working set 3 GB > L2"}
+
+
+def ensemble_cost(pkg, device: int, systems: int = 1024, steps: int = 100,
+                  loop_steps: int = 10) -> dict:
+    """Batched ensemble: 1,024 systems, sizes log-uniform in [1024, 262144],
+    Plummer projection (a = 0.1) or uniform disk 50/50, theta 0.5, eps 1e-3,
+    dt 1e-4, leapfrog; `steps` steps of the whole ensemble (one launch per
+    stage, one graph per step, autotuned) against looping the single-system
+    solver over the same systems (each system its own handle and stream, all
+    systems issued back to back per step with no host sync, graphs on).  Both
+    sides are timed with CUDA events after warm-up; the loop is timed over
+    `loop_steps` steps."""
+    import torch
+    cfg = pkg.Config(bhTheta=0.5, deltaTime=1e-4, softening="plummer", plummerEps=1e-3,
+                     mortonDomain="bbox", integrator="leapfrog-kdk", walk="group", leafSize=8)
+    sizes = pkg.ensemble_sizes(systems, 2024, 1024, 262144)
+    total = int(sizes.sum())
+    dev = torch.device("cuda", device)
+    ens = pkg.Ensemble(sizes, cfg, device=device)
+    ens.setScenarios(None, seed=2024)
+    mass, pos, vel = ens.download()
+    tune = ens.autotune(2)
+    tuned = ens.config
+    for _ in range(3):
+        ens.step(1)
+    ens.sync()
+    ext = torch.cuda.ExternalStream(ens.getBuffers().stream, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ens.profile_begin(steps)
+    e0.record(ext)
+    ens.step(steps)
+    e1.record(ext)
+    ens.sync()
+    stage_ms, rec = ens.profile_end()
+    ens_ms = e0.elapsed_time(e1) / steps
+    acc = ens.computeAccelerations()
+    m2, p2, _ = ens.download()
+    # force error on a sample of systems (each against its own FP64 direct sum)
+    off = ens.offsets
+    rng = np.random.default_rng(1)
+    errs = []
+    for k in rng.choice(systems, 16, replace=False):
+        sl = slice(int(off[k]), int(off[k + 1]))
+        med, p99, ns = force_error_vs_fp64(acc[sl], m2[sl], p2[sl], cfg, nsample=16, seed=int(k))
+        errs.append(med)
+    kps = ens.kernels_per_step()
+    ens.close()
+
+    # looped single-system solver over the same systems and initial states,
+    # each system its own handle (tuned walk parameters, graphs on)
+    sims = []
+    for k in range(systems):
+        sl = slice(int(off[k]), int(off[k + 1]))
+        sim = pkg.Simulation(tuned, device=device)
+        sim.setNumBodies(int(sizes[k]))
+        sim.upload(mass[sl], pos[sl], vel[sl])
+        sims.append(sim)
+    for sim in sims:
+        sim.step(2)
+    torch.cuda.synchronize(dev)
+    # (a) system by system: each system's steps, then the next system
+    t0 = time.perf_counter()
+    for sim in sims:
+        sim.step(loop_steps)
+        sim.sync()
+    seq_ms = (time.perf_counter() - t0) * 1e3 / loop_steps
+    # (b) all systems issued back to back per step on their own streams
+    t0 = time.perf_counter()
+    for _ in range(loop_steps):
+        for sim in sims:
+            sim.step(1)
+    for sim in sims:
+        sim.sync()
+    conc_ms = (time.perf_counter() - t0) * 1e3 / loop_steps
+    for sim in sims:
+        sim.close()
+    return {"systems": systems, "bodies": total, "steps": steps,
+            "sizes": {"min": int(sizes.min()), "max": int(sizes.max()),
+                      "median": float(np.median(sizes))},
+            "value": total / (ens_ms / 1e3), "unit": "body-steps/s", "ms_per_step": ens_ms,
+            "stages_ms": {k: v / max(rec, 1) for k, v in stage_ms.items()},
+            "kernels_per_step": kps, "autotune": tune,
+            "force_error_vs_fp64_median_of_system_medians": float(np.median(errs)),
+            "loop_ms_per_step": seq_ms, "loop_value": total / (seq_ms / 1e3),
+            "speedup_vs_loop": seq_ms / ens_ms,
+            "concurrent_loop_ms_per_step": conc_ms, "speedup_vs_concurrent_loop": conc_ms / ens_ms,
+            "timing": "ensemble: CUDA events on the engine stream; loops: host clock around "
+                      "synchronised calls (one handle and stream per system), same systems "
+                      "and states"}
 
 
 # ---------------------------------------------------------------- helpers
@@ -458,6 +549,8 @@ def run_own(args):
             out["secondary"] = secondary_16m(pkg, local)
         if not args.no_adjoint:
             out["adjoint"] = adjoint_cost(pkg, local)
+        if not args.no_ensemble:
+            out["ensemble"] = ensemble_cost(pkg, local)
         print(json.dumps(out))
     if dist is not None:
         dist.barrier()

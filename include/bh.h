@@ -231,6 +231,31 @@ int bh_rollout_grad(bh_sim* sim, uint32_t steps, uint32_t checkpoint_every,
                     const float* target_pos, float* loss, float* grad_pos, float* grad_vel,
                     float* grad_mass);
 
+/* ---- batched ensembles (extension; no reference counterpart) ------------- */
+/* An ensemble handle advances many independent systems with one launch per
+ * stage: the bodies of all systems are concatenated (system k owns bodies
+ * [off_k, off_k+1)), each system gets its own bounding box and 32-bit Morton
+ * domain, the sort keys are (system << 32) | code so one sort and one
+ * hierarchy build serve every system (the tree's top levels split by
+ * system), and each walk group only interacts with its own system.  All
+ * other calls (bh_step, bh_upload, bh_download, bh_get_buffers, ...) work on
+ * the concatenation.  Needs walk_mode BH_WALK_GROUP and morton_bits 32; every
+ * system has at least 256 bodies. */
+int bh_ensemble_create(const bh_config* config, const uint32_t* bodies_per_system,
+                       uint32_t num_systems, bh_sim** out);
+
+/* Fill every system: names[k] is system k's scenario (seed derived from
+ * `seed` and k); names == NULL picks a Plummer-sphere projection (scale
+ * radius 0.1) or a uniform disk with probability 1/2 each. */
+int bh_ensemble_set_scenarios(bh_sim* sim, const char* const* names, uint64_t seed);
+
+/* Log-uniform system sizes in [min_bodies, max_bodies] from PCG32(seed). */
+int bh_ensemble_sizes(uint32_t num_systems, uint64_t seed, uint32_t min_bodies,
+                      uint32_t max_bodies, uint32_t* out);
+
+int bh_get_num_systems(bh_sim* sim, uint32_t* out);       /* 0 for a single system */
+int bh_get_system_offsets(bh_sim* sim, uint32_t* offsets); /* num_systems + 1 entries */
+
 /* ---- allocation-free hierarchy build ------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot let this library
  * allocate device memory (a host that plans the whole GPU heap and hands out

@@ -7,5 +7,5 @@ repository root on ``sys.path``.
 """
 from ._lib import BhError, load  # noqa: F401
 from .config import WORKLOADS, Config, getDefaultConfig  # noqa: F401
-from .simulation import (SCENARIOS, CommandBuffer, SimBuffers, Simulation,  # noqa: F401
-                         generate_scenario, submit)
+from .simulation import (SCENARIOS, CommandBuffer, Ensemble, SimBuffers,  # noqa: F401
+                         Simulation, ensemble_sizes, generate_scenario, submit)

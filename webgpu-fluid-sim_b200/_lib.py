@@ -113,6 +113,13 @@ SIGNATURES = {
     "bh_walk_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_uint64)]),
+    "bh_ensemble_create": (ctypes.c_int, [ctypes.POINTER(bh_config), _P, ctypes.c_uint32,
+                                          ctypes.POINTER(_P)]),
+    "bh_ensemble_set_scenarios": (ctypes.c_int, [_P, _P, ctypes.c_uint64]),
+    "bh_ensemble_sizes": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32,
+                                         ctypes.c_uint32, _P]),
+    "bh_get_num_systems": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint32)]),
+    "bh_get_system_offsets": (ctypes.c_int, [_P, _P]),
     "bh_autotune": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(bh_tune_result)]),
     "bh_get_config": (ctypes.c_int, [_P, ctypes.POINTER(bh_config)]),
     "bh_force_vjp": (ctypes.c_int, [_P, _P, _P, _P]),

@@ -70,6 +70,9 @@ struct WalkParams {
     int multipole;    // 1 or 2
     int bpl;          // bodies per lane
     unsigned int* group_ctr;  // dynamic group counter (zeroed per step)
+    // ensemble: a group only sees its own system's slot range
+    uint32_t num_systems;
+    const uint32_t* sys_off;
 };
 
 // Per-step scratch that must start at zero.  One memset clears it.
@@ -112,6 +115,12 @@ struct DeviceBuffers {
     uint32_t* status = nullptr;  // look-back status: passes * tiles * 256
     uint32_t tiles = 0;
     uint32_t* err = nullptr;     // device error word
+    int sort_passes = 0;         // 0: one per key byte; ensembles sort fewer (even count)
+    // ensemble of independent systems (num_systems = 0: one system)
+    uint32_t num_systems = 0;
+    const uint32_t* sys_off = nullptr;  // E+1 body offsets (original order = sorted order by system)
+    const uint32_t* body_sys = nullptr; // n: system of each body (original order)
+    uint32_t* sys_bbox = nullptr;       // 4E ordered-int max of {-minx, -miny, maxx, maxy}
 };
 
 // ---- launchers (all asynchronous on `s`) --------------------------------
@@ -121,6 +130,9 @@ void launch_bbox(const DeviceBuffers& b, cudaStream_t s);
 void launch_encode(const DeviceBuffers& b, int domain, cudaStream_t s);
 // leapfrog opening kick + drift: v += a*hdt; x += v*dt (original order)
 void launch_kick_drift(const DeviceBuffers& b, float dt, cudaStream_t s);
+// ensemble: per-system boxes, and keys (system << 32) | morton32(system box)
+void launch_bbox_ensemble(const DeviceBuffers& b, cudaStream_t s);
+void launch_encode_ensemble(const DeviceBuffers& b, cudaStream_t s);
 // sort.cu
 void launch_sort(const DeviceBuffers& b, cudaStream_t s);
 cudaError_t sort_init_attributes();

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -55,6 +56,8 @@ struct bh_sim {
         float *mbar_slot = nullptr, *mbar = nullptr;
         double* loss = nullptr;
     } adj;
+    // ensemble of independent systems (empty: one system)
+    std::vector<uint32_t> sys_sizes;
     std::string err;
 };
 
@@ -173,7 +176,9 @@ struct Carver {
 
 static int alloc_buffers(bh_sim* s, uint32_t n) {
     free_buffers(s);
-    const int kb = s->cfg.morton_bits / 8;
+    const uint32_t E = (uint32_t)s->sys_sizes.size();
+    // Ensembles key (system << 32) | 32-bit Morton code: 64-bit keys.
+    const int kb = E ? 8 : s->cfg.morton_bits / 8;
     const size_t nn = n ? 2 * (size_t)n - 1 : 1, ni = n > 1 ? (size_t)n - 1 : 1, nb = n ? n : 1;
     const uint32_t tiles = (uint32_t)((n + bh::kSortTile - 1) / bh::kSortTile);
     Carver c;
@@ -190,6 +195,8 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     size_t o_scr = c.take<bh::StepScratch>(1);
     size_t o_status = c.take<uint32_t>((size_t)kb * (tiles ? tiles : 1) * bh::kRadix);
     size_t o_err = c.take<uint32_t>(1);
+    size_t o_soff = E ? c.take<uint32_t>(E + 1) : 0, o_bsys = E ? c.take<uint32_t>(nb) : 0;
+    size_t o_sbox = E ? c.take<uint32_t>(4 * (size_t)E) : 0;
     void* arena = nullptr;
     cudaError_t e = cudaMalloc(&arena, c.off);
     if (e != cudaSuccess) {
@@ -228,6 +235,26 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     b.err = (uint32_t*)(a + o_err);
     BH_CUDA(s, cudaMemsetAsync(arena, 0, c.off, s->stream));
     BH_CUDA(s, cudaMemsetAsync(b.bound, 0xFF, sizeof(uint32_t) * ni, s->stream));
+    if (E) {
+        // offsets and per-body system ids (systems are contiguous)
+        std::vector<uint32_t> off(E + 1, 0), bsys(nb, 0);
+        for (uint32_t k = 0; k < E; ++k) {
+            off[k + 1] = off[k] + s->sys_sizes[k];
+            for (uint32_t i = off[k]; i < off[k + 1]; ++i) bsys[i] = k;
+        }
+        b.num_systems = E;
+        b.sys_off = (uint32_t*)(a + o_soff);
+        b.body_sys = (uint32_t*)(a + o_bsys);
+        b.sys_bbox = (uint32_t*)(a + o_sbox);
+        // key bits = 32 + bits of the largest system id; an even pass count
+        // lands the sorted keys back in `codes`
+        int sb = 0;
+        while (sb < 32 && ((E - 1) >> sb)) ++sb;
+        int passes = (32 + sb + 7) / 8;
+        b.sort_passes = passes + (passes & 1);
+        BH_CUDA(s, cudaMemcpy((void*)b.sys_off, off.data(), 4 * (size_t)(E + 1), cudaMemcpyHostToDevice));
+        BH_CUDA(s, cudaMemcpy((void*)b.body_sys, bsys.data(), 4 * (size_t)nb, cudaMemcpyHostToDevice));
+    }
     BH_CUDA(s, cudaStreamSynchronize(s->stream));
     s->acc_valid = false;
     return BH_OK;
@@ -253,6 +280,8 @@ static bh::WalkParams walk_params(const bh_sim* s, int mode) {
     p.multipole = c.multipole_order;
     p.bpl = c.bodies_per_lane > 0 ? c.bodies_per_lane : 2;
     p.group_ctr = s->b.scratch ? s->b.scratch->group_ctr : nullptr;
+    p.num_systems = s->b.num_systems;
+    p.sys_off = s->b.sys_off;
     return p;
 }
 
@@ -272,8 +301,14 @@ static void enqueue_tree_on(bh_sim* s, const DeviceBuffers& b, Mark mark) {
     cudaMemsetAsync(b.scratch, 0, sizeof(bh::StepScratch), st);
     cudaMemsetAsync(b.status, 0, sizeof(uint32_t) * (size_t)b.key_bytes * b.tiles * bh::kRadix, st);
     mark(1);
-    if (needs_bbox(s)) bh::launch_bbox(b, st);
-    bh::launch_encode(b, s->cfg.morton_domain, st);
+    if (b.num_systems > 0) {
+        cudaMemsetAsync(b.sys_bbox, 0, sizeof(uint32_t) * 4 * (size_t)b.num_systems, st);
+        bh::launch_bbox_ensemble(b, st);
+        bh::launch_encode_ensemble(b, st);
+    } else {
+        if (needs_bbox(s)) bh::launch_bbox(b, st);
+        bh::launch_encode(b, s->cfg.morton_domain, st);
+    }
     mark(2);
     bh::launch_sort(b, st);
     mark(3);
@@ -379,12 +414,56 @@ static int check_device_errors(bh_sim* s) {
 
 // ---- lifetime ------------------------------------------------------------------
 
+static int create_sim(const bh_config* config, const uint32_t* sizes, uint32_t num_systems,
+                      bh_sim** out);
+
 extern "C" int bh_create(const bh_config* config, bh_sim** out) {
+    return create_sim(config, nullptr, 0, out);
+}
+
+// Smallest system of an ensemble: larger than the biggest walk group (4 x 32),
+// so no group can hold bodies of two systems (a subtree holding parts of two
+// systems holds both of them whole).
+static constexpr uint32_t kMinSystemBodies = 256;
+
+extern "C" int bh_ensemble_create(const bh_config* config, const uint32_t* bodies_per_system,
+                                  uint32_t num_systems, bh_sim** out) {
+    if (!bodies_per_system || num_systems == 0)
+        return fail(nullptr, BH_ERR_INVALID_ARGUMENT, "bh_ensemble_create: no systems");
+    if (num_systems > (1u << 24))
+        return fail(nullptr, BH_ERR_INVALID_ARGUMENT, "bh_ensemble_create: at most 2^24 systems");
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < num_systems; ++k) {
+        if (bodies_per_system[k] < kMinSystemBodies)
+            return fail(nullptr, BH_ERR_INVALID_ARGUMENT,
+                        "bh_ensemble_create: every system needs at least 256 bodies");
+        total += bodies_per_system[k];
+    }
+    if (total > kMaxBodies)
+        return fail(nullptr, BH_ERR_INVALID_ARGUMENT, "bh_ensemble_create: more than 2^30 - 1 bodies");
+    bh_config c;
+    if (config) c = *config;
+    else bh_default_config(&c);
+    if (c.walk_mode != BH_WALK_GROUP || c.morton_bits != 32)
+        return fail(nullptr, BH_ERR_NOT_SUPPORTED,
+                    "ensembles need the group walk and 32-bit Morton codes per system");
+    return create_sim(&c, bodies_per_system, num_systems, out);
+}
+
+static int create_sim(const bh_config* config, const uint32_t* sizes, uint32_t num_systems,
+                      bh_sim** out) {
     if (!out) return fail(nullptr, BH_ERR_INVALID_ARGUMENT, "bh_create: null output");
     *out = nullptr;
     bh_sim* s = new bh_sim();
     if (config) s->cfg = *config;
     else bh_default_config(&s->cfg);
+    if (num_systems) {
+        s->sys_sizes.assign(sizes, sizes + num_systems);
+        uint64_t total = 0;
+        for (uint32_t k = 0; k < num_systems; ++k) total += sizes[k];
+        s->n = (uint32_t)total;
+        s->scenario = "";
+    }
     int rc = validate_config(s, s->cfg);
     if (rc != BH_OK) {
         delete s;
@@ -482,6 +561,8 @@ static int load_scenario(bh_sim* s, const std::string& name, uint64_t seed, uint
 
 extern "C" int bh_set_num_bodies(bh_sim* s, uint32_t n) {
     BH_HANDLE(s);
+    if (!s->sys_sizes.empty())
+        return fail(s, BH_ERR_NOT_SUPPORTED, "an ensemble's body counts are fixed at creation");
     if (n > kMaxBodies) return fail(s, BH_ERR_INVALID_ARGUMENT, "body count above 2^30 - 1");
     return load_scenario(s, s->scenario, s->seed, n);  // simulation.ts:227-231
 }
@@ -489,7 +570,72 @@ extern "C" int bh_set_num_bodies(bh_sim* s, uint32_t n) {
 extern "C" int bh_set_scenario(bh_sim* s, const char* name, uint64_t seed) {
     BH_HANDLE(s);
     if (!name) return fail(s, BH_ERR_INVALID_ARGUMENT, "null scenario name");
+    if (!s->sys_sizes.empty())
+        return fail(s, BH_ERR_NOT_SUPPORTED, "use bh_ensemble_set_scenarios on an ensemble");
     return load_scenario(s, name, seed, s->n);
+}
+
+// ---- ensembles (extension) ------------------------------------------------------
+
+namespace bh {
+double pcg_uniform(uint64_t seed, uint64_t stream, uint32_t draw);
+}
+
+extern "C" int bh_ensemble_sizes(uint32_t num_systems, uint64_t seed, uint32_t min_bodies,
+                                 uint32_t max_bodies, uint32_t* out) {
+    if (!out || num_systems == 0 || min_bodies == 0 || max_bodies < min_bodies)
+        return fail(nullptr, BH_ERR_INVALID_ARGUMENT, "bh_ensemble_sizes: bad arguments");
+    const double lo = std::log((double)min_bodies), hi = std::log((double)max_bodies);
+    for (uint32_t k = 0; k < num_systems; ++k) {
+        const double u = bh::pcg_uniform(seed, k, 0);
+        uint32_t v = (uint32_t)std::floor(std::exp(lo + (hi - lo) * u));
+        out[k] = v < min_bodies ? min_bodies : (v > max_bodies ? max_bodies : v);
+    }
+    return BH_OK;
+}
+
+extern "C" int bh_ensemble_set_scenarios(bh_sim* s, const char* const* names, uint64_t seed) {
+    BH_HANDLE(s);
+    const uint32_t E = (uint32_t)s->sys_sizes.size();
+    if (E == 0) return fail(s, BH_ERR_NOT_SUPPORTED, "not an ensemble");
+    const size_t n = s->b.n;
+    std::vector<float> mass(n), pos(2 * n), vel(2 * n), rad(n);
+    size_t off = 0;
+    for (uint32_t k = 0; k < E; ++k) {
+        // Per system: its own seed; without names, a Plummer-sphere projection
+        // (scale radius 0.1) or a uniform disk, chosen 50/50.
+        const uint64_t sk = seed * 0x9E3779B97F4A7C15ULL + k;
+        const char* nm = names ? names[k]
+                               : (bh::pcg_uniform(seed, k, 1) < 0.5 ? "plummer-projection"
+                                                                   : "uniform-disk-kepler");
+        if (!nm || bh::generate_scenario(nm, s->sys_sizes[k], sk, s->cfg.grav_constant,
+                                         mass.data() + off, pos.data() + 2 * off,
+                                         vel.data() + 2 * off, rad.data() + off) != 0)
+            return fail(s, BH_ERR_UNKNOWN_SCENARIO,
+                        std::string("Unknown scenario: ") + (nm ? nm : "(null)"));
+        off += s->sys_sizes[k];
+    }
+    BH_CUDA(s, cudaMemcpyAsync(s->b.mass, mass.data(), 4 * n, cudaMemcpyHostToDevice, s->stream));
+    BH_CUDA(s, cudaMemcpyAsync(s->b.pos, pos.data(), 8 * n, cudaMemcpyHostToDevice, s->stream));
+    BH_CUDA(s, cudaMemcpyAsync(s->b.vel, vel.data(), 8 * n, cudaMemcpyHostToDevice, s->stream));
+    BH_CUDA(s, cudaMemcpyAsync(s->b.radius, rad.data(), 4 * n, cudaMemcpyHostToDevice, s->stream));
+    BH_CUDA(s, cudaStreamSynchronize(s->stream));
+    s->acc_valid = false;
+    return BH_OK;
+}
+
+extern "C" int bh_get_num_systems(bh_sim* s, uint32_t* out) {
+    if (!s || !out) return fail(s, BH_ERR_INVALID_ARGUMENT, "null argument");
+    *out = (uint32_t)s->sys_sizes.size();
+    return BH_OK;
+}
+
+extern "C" int bh_get_system_offsets(bh_sim* s, uint32_t* out) {
+    if (!s || !out) return fail(s, BH_ERR_INVALID_ARGUMENT, "null argument");
+    uint32_t acc = 0;
+    out[0] = 0;
+    for (size_t k = 0; k < s->sys_sizes.size(); ++k) out[k + 1] = (acc += s->sys_sizes[k]);
+    return BH_OK;
 }
 
 extern "C" int bh_update_metadata(bh_sim* s) {
@@ -597,6 +743,8 @@ static int adjoint_supported(bh_sim* s) {
     if (s->cfg.walk_mode != BH_WALK_GROUP || s->cfg.softening != BH_SOFTENING_PLUMMER)
         return fail(s, BH_ERR_NOT_SUPPORTED,
                     "the adjoint needs the group walk and Plummer softening");
+    if (s->b.num_systems > 0)
+        return fail(s, BH_ERR_NOT_SUPPORTED, "the adjoint runs on single systems, not ensembles");
     return BH_OK;
 }
 
@@ -928,7 +1076,7 @@ extern "C" int bh_kernels_per_step(bh_sim* s, uint32_t* out) {
     if (!s || !out) return fail(s, BH_ERR_INVALID_ARGUMENT, "null argument");
     uint32_t k = 0;
     if (s->cfg.integrator == BH_INTEGRATOR_LEAPFROG_KDK) k += 1;  // kick + drift
-    if (needs_bbox(s)) k += 1;                                      // bbox
+    if (needs_bbox(s) || s->b.num_systems) k += 1;                 // bbox (per system)
     k += 1;                                                         // encode
     k += (uint32_t)bh::sort_passes(s->b);                          // sort passes
     k += 1;                                                         // build + fill

@@ -204,6 +204,98 @@ void launch_encode(const DeviceBuffers& b, int domain, cudaStream_t s) {
         encode_kernel<uint32_t><<<blocks, 256, 0, s>>>(p2, b.n, (uint32_t*)b.codes, domain, b.scratch);
 }
 
+// ---- ensembles: one box and one 32-bit Morton domain per system ----------
+// A warp whose 32 bodies all belong to one system (the common case: systems
+// are contiguous) reduces first and issues one atomic per bound.
+__global__ void __launch_bounds__(256) bbox_ensemble_kernel(const float2* __restrict__ pos,
+                                                            const uint32_t* __restrict__ body_sys,
+                                                            uint32_t n, uint32_t* __restrict__ sys_bbox) {
+    const unsigned FULL = 0xFFFFFFFFu;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const bool ok = i < n;
+        const float2 p = ok ? __ldg(&pos[i]) : make_float2(0.f, 0.f);
+        const uint32_t sys = ok ? __ldg(&body_sys[i]) : kSentinel;
+        float v[4] = {ok ? -p.x : -INFINITY, ok ? -p.y : -INFINITY, ok ? p.x : -INFINITY,
+                      ok ? p.y : -INFINITY};
+        const uint32_t s0 = __shfl_sync(FULL, sys, 0);
+        if (__all_sync(FULL, !ok || sys == s0)) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v[k] = fmaxf(v[k], __shfl_xor_sync(FULL, v[k], o));
+            if ((threadIdx.x & 31) == 0 && s0 != kSentinel)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) atomicMax(&sys_bbox[4 * s0 + k], f2ord(v[k]));
+        } else if (ok) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) atomicMax(&sys_bbox[4 * sys + k], f2ord(v[k]));
+        }
+    }
+}
+
+void launch_bbox_ensemble(const DeviceBuffers& b, cudaStream_t s) {
+    if (b.n == 0) return;
+    int blocks = (int)((b.n + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    bbox_ensemble_kernel<<<blocks, 256, 0, s>>>(b.pos, b.body_sys, b.n, b.sys_bbox);
+}
+
+// key = (system << 32) | morton32 over the system's box (same quantisation as
+// the single-system bbox domain); histograms of the sort's digit passes.
+__global__ void __launch_bounds__(256) encode_ensemble_kernel(const float2* __restrict__ pos,
+                                                              const uint32_t* __restrict__ body_sys,
+                                                              const uint32_t* __restrict__ sys_bbox,
+                                                              uint32_t n, int passes,
+                                                              uint64_t* __restrict__ codes,
+                                                              StepScratch* scratch) {
+    __shared__ uint32_t sh[8][kRadix];
+    for (int i = threadIdx.x; i < 8 * kRadix; i += blockDim.x) (&sh[0][0])[i] = 0;
+    __syncthreads();
+    const unsigned FULL = 0xFFFFFFFFu;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const bool ok = i < n;
+        uint64_t k = 0;
+        if (ok) {
+            const float2 p = __ldg(&pos[i]);
+            const uint32_t sys = __ldg(&body_sys[i]);
+            const float mnx = -ord2f(__ldg(&sys_bbox[4 * sys])), mny = -ord2f(__ldg(&sys_bbox[4 * sys + 1]));
+            const float mxx = ord2f(__ldg(&sys_bbox[4 * sys + 2])), mxy = ord2f(__ldg(&sys_bbox[4 * sys + 3]));
+            float ext = fmaxf(__fsub_rn(mxx, mnx), __fsub_rn(mxy, mny));
+            if (!(ext > 0.0f)) ext = 1.0f;
+            const uint32_t m = spread16(quant16(p.x, mnx, ext)) | (spread16(quant16(p.y, mny, ext)) << 1);
+            k = ((uint64_t)sys << 32) | m;
+            codes[i] = k;
+        }
+        // Morton digits are spread out: one shared atomic per body.  System
+        // digits repeat across a warp: one atomic per distinct digit.
+        const unsigned act = __ballot_sync(FULL, ok);
+        for (int q = 0; q < 4 && q < passes; ++q)
+            if (ok) atomicAdd(&sh[q][(uint32_t)(k >> (8 * q)) & 0xFFu], 1u);
+        for (int q = 4; q < passes; ++q) {
+            if (ok) {
+                const uint32_t d = (uint32_t)(k >> (8 * q)) & 0xFFu;
+                const unsigned peers = __match_any_sync(act, d);
+                if ((threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) atomicAdd(&sh[q][d], (uint32_t)__popc(peers));
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x) {
+        const uint32_t c = (&sh[0][0])[i];
+        if (c) atomicAdd(&scratch->hist[i / kRadix][i % kRadix], c);
+    }
+}
+
+void launch_encode_ensemble(const DeviceBuffers& b, cudaStream_t s) {
+    if (b.n == 0) return;
+    int blocks = (int)((b.n + 255) / 256);
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    encode_ensemble_kernel<<<blocks, 256, 0, s>>>(b.pos, b.body_sys, b.sys_bbox, b.n, b.sort_passes,
+                                                  (uint64_t*)b.codes, b.scratch);
+}
+
 // ---- leapfrog opening kick + drift (original order, coalesced) -----------
 __global__ void __launch_bounds__(256) kick_drift_kernel(float2* __restrict__ pos,
                                                          float2* __restrict__ vel,

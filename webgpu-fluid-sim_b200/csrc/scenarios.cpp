@@ -216,6 +216,15 @@ static void gen_plummer_projection(uint32_t n, Pcg32& rng, double G, float* mass
     }
 }
 
+// Draw `draw` of stream `stream` of a PCG32 seeded with `seed` (ensemble
+// sizes and per-system scenario choices).
+double pcg_uniform(uint64_t seed, uint64_t stream, uint32_t draw) {
+    Pcg32 rng(seed, 0x5851f42d4c957f2dULL + 2 * stream);
+    double u = rng.uniform();
+    for (uint32_t k = 0; k < draw; ++k) u = rng.uniform();
+    return u;
+}
+
 // Returns 0 on success, -1 for an unknown name.
 int generate_scenario(const char* name, uint32_t n, uint64_t seed, float grav_constant,
                       float* mass, float* pos, float* vel, float* radius_mul) {

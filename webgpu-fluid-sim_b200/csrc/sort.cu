@@ -182,12 +182,14 @@ onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_
     }
 }
 
-int sort_passes(const DeviceBuffers& b) { return b.key_bytes; }
+// One pass per key byte, or fewer (an even count) when the high bytes are
+// known to be zero (ensemble keys: system id above a 32-bit Morton code).
+int sort_passes(const DeviceBuffers& b) { return b.sort_passes > 0 ? b.sort_passes : b.key_bytes; }
 
 template <typename K>
 static void sort_impl(const DeviceBuffers& b, cudaStream_t s) {
     const size_t smem = (size_t)kSortTile * (sizeof(K) + sizeof(uint32_t));
-    const int passes = (int)sizeof(K);
+    const int passes = sort_passes(b);
     K* kin = (K*)b.codes;
     K* kout = (K*)b.codes_alt;
     uint32_t* iin = b.ids;

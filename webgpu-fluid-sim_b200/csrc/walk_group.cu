@@ -130,6 +130,19 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
         const uint2 grp = __ldg(&groups[g]);
         const uint32_t base = grp.x, nvalid = grp.y;
         const int kmax = (int)((nvalid + 31u) / 32u);  // sub-slots in use (uniform)
+        // Ensemble: the slot range of this group's system (systems stay
+        // contiguous in sorted order because the system id tops every key).
+        uint32_t sys_lo = 0, sys_hi = n;
+        if (P.num_systems > 0) {
+            uint32_t lo = 0, hi = P.num_systems;  // sys_off[lo] <= base < sys_off[hi]
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (__ldg(&P.sys_off[mid]) <= base) lo = mid;
+                else hi = mid;
+            }
+            sys_lo = __ldg(&P.sys_off[lo]);
+            sys_hi = __ldg(&P.sys_off[lo + 1]);
+        }
         float bx[BPL], by[BPL], bm[BPL];
         float glox = INFINITY, gloy = INFINITY, ghix = -INFINITY, ghiy = -INFINITY;
 #pragma unroll
@@ -286,7 +299,7 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
             float4 mom = make_float4(0.f, 0.f, 0.f, 0.f), sq = mom;
             if (has) {
                 if (v >= nm1) {
-                    emit_range = true;
+                    emit_range = (v - nm1) >= sys_lo && (v - nm1) < sys_hi;
                     r0 = v - nm1;
                     r1 = 1;
                 } else {
@@ -300,7 +313,14 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
                     const float dy = fmaxf(0.0f, fmaxf(__fsub_rn(box.y, ghiy), __fsub_rn(gloy, box.w)));
                     const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
                     const float L = fmaxf(__fsub_rn(box.z, box.x), __fsub_rn(box.w, box.y));
-                    if (__fmul_rn(L, L) < __fmul_rn(th2, d2)) {
+                    const uint32_t f = lk.z, e = lk.z + lk.w;
+                    if (e <= sys_lo || f >= sys_hi) {
+                        // another system's subtree: no interaction
+                    } else if (f < sys_lo || e > sys_hi) {
+                        push = true;  // spans several systems: always open
+                        r0 = lk.x;
+                        r1 = lk.y;
+                    } else if (__fmul_rn(L, L) < __fmul_rn(th2, d2)) {
                         emit_node = true;
                         mom = m4;
                         sq = q4;

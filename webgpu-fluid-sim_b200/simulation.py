@@ -281,3 +281,60 @@ def generate_scenario(name: str, n: int, seed: int = 0, grav_constant: float = 1
         raise _lib.BhError(st, f"Unknown scenario: {name}")
     _lib.check(st)
     return mass, pos, vel, rad
+
+
+def ensemble_sizes(num_systems: int, seed: int, min_bodies: int, max_bodies: int) -> np.ndarray:
+    """Log-uniform system sizes in [min_bodies, max_bodies] (PCG32 stream)."""
+    lib = _lib.load()
+    out = np.empty(num_systems, np.uint32)
+    _lib.check(lib.bh_ensemble_sizes(num_systems, seed, min_bodies, max_bodies, _ptr(out)))
+    return out
+
+
+class Ensemble(Simulation):
+    """Many independent systems advanced by one launch per stage.
+
+    The bodies of all systems are concatenated (system k owns
+    ``offsets[k]:offsets[k+1]``); every Simulation call (step, upload,
+    download, getBuffers, computeAccelerations, ...) acts on the
+    concatenation.  setNumBodies / setScenario have no meaning for an
+    ensemble and raise; use ``setScenarios``.
+    """
+
+    def __init__(self, sizes, config: Config | None = None, device: int = 0):
+        self.config = config or getDefaultConfig()
+        self._lib = _lib.load()
+        c = self.config.to_c(device)
+        sz = np.ascontiguousarray(sizes, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.bh_ensemble_create(ctypes.byref(c), _ptr(sz), int(sz.size),
+                                                ctypes.byref(h)))
+        self._h = h
+        self.device = device
+        self.currentScenario = "ensemble"
+        self.seed = 0
+        self.sizes = sz.copy()
+        self.offsets = np.zeros(sz.size + 1, np.uint32)
+        self._check(self._lib.bh_get_system_offsets(self._h, _ptr(self.offsets)))
+
+    def setScenarios(self, names=None, seed: int = 0) -> None:
+        """names[k] = scenario of system k; None = Plummer projection (a=0.1)
+        or uniform disk, 1/2 each, per system."""
+        self.seed = int(seed)
+        if names is None:
+            self._check(self._lib.bh_ensemble_set_scenarios(self._h, None, self.seed))
+            return
+        if len(names) != self.sizes.size:
+            raise ValueError(f"expected {self.sizes.size} scenario names, got {len(names)}")
+        enc = [n.encode() for n in names]
+        arr = (ctypes.c_char_p * len(enc))(*enc)
+        st = self._lib.bh_ensemble_set_scenarios(self._h, ctypes.cast(arr, ctypes.c_void_p),
+                                                 self.seed)
+        if st == _lib.BH_ERR_UNKNOWN_SCENARIO:
+            raise _lib.BhError(st, "Unknown scenario in ensemble")
+        self._check(st)
+
+    def numSystems(self) -> int:
+        k = ctypes.c_uint32()
+        self._check(self._lib.bh_get_num_systems(self._h, ctypes.byref(k)))
+        return int(k.value)
