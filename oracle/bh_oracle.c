@@ -535,11 +535,16 @@ void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const 
                 const uint32_t v = stack[--sp];
                 if (v >= nm1) { rfirst[nr] = v - nm1; rcount[nr++] = 1; continue; }
                 const float* bx = &aabb[4 * (size_t)v];
-                const float dx = fmaxf(0.0f, fmaxf(bx[0] - hix, lox - bx[2]));
-                const float dy = fmaxf(0.0f, fmaxf(bx[1] - hiy, loy - bx[3]));
+                const float cx = com[2 * (size_t)v], cy = com[2 * (size_t)v + 1];
+                /* accept: size L < theta x distance from the group's box to the
+                 * node's COM, and the two boxes apart */
+                const float dx = fmaxf(0.0f, fmaxf(cx - hix, lox - cx));
+                const float dy = fmaxf(0.0f, fmaxf(cy - hiy, loy - cy));
                 const float d2 = dx * dx + dy * dy;
                 const float Ls = fmaxf(bx[2] - bx[0], bx[3] - bx[1]);
-                if (Ls * Ls < th2 * d2) {
+                const float sx = fmaxf(bx[0] - hix, lox - bx[2]);
+                const float sy = fmaxf(bx[1] - hiy, loy - bx[3]);
+                if (Ls * Ls < th2 * d2 && (sx > 0.0f || sy > 0.0f)) {
                     nodes[nn_++] = v;
                 } else if (last[v] - first[v] + 1 <= L) {
                     rfirst[nr] = first[v];

@@ -223,11 +223,7 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
                     const uint4 lk = __ldg(&gnode[v].link);
                     mom = __ldg(&gnode[v].mom);
                     if (MP >= 2) sq = __ldg(&gnode[v].quad);
-                    const float dx = fmaxf(0.0f, fmaxf(__fsub_rn(box.x, ghix), __fsub_rn(glox, box.z)));
-                    const float dy = fmaxf(0.0f, fmaxf(__fsub_rn(box.y, ghiy), __fsub_rn(gloy, box.w)));
-                    const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-                    const float L = fmaxf(__fsub_rn(box.z, box.x), __fsub_rn(box.w, box.y));
-                    if (__fmul_rn(L, L) < __fmul_rn(th2, d2)) {
+                    if (group_accepts(box, mom.x, mom.y, glox, gloy, ghix, ghiy, th2)) {
                         emit_node = true;
                     } else if (lk.w <= (uint32_t)P.leaf_size) {
                         emit_range = true;

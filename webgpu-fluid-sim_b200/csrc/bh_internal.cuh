@@ -39,6 +39,23 @@ struct __align__(16) GNode {
     uint4 link;   // {left, right, first slot, body count}
 };
 
+// Group acceptance test.  A node stands in for its bodies, as one multipole,
+// for a whole group when its size L and the distance d from the group's box
+// to the node's centre of mass satisfy L < theta d -- then every body of the
+// group meets the per-body test length / d_body < theta -- and the node's box
+// lies apart from the group's box.  Every operation rounds to nearest (no
+// contraction), so a CPU restatement reproduces each decision.
+__device__ __forceinline__ bool group_accepts(const float4& box, float cx, float cy, float glox,
+                                              float gloy, float ghix, float ghiy, float th2) {
+    const float dx = fmaxf(0.0f, fmaxf(__fsub_rn(cx, ghix), __fsub_rn(glox, cx)));
+    const float dy = fmaxf(0.0f, fmaxf(__fsub_rn(cy, ghiy), __fsub_rn(gloy, cy)));
+    const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+    const float L = fmaxf(__fsub_rn(box.z, box.x), __fsub_rn(box.w, box.y));
+    const float sx = fmaxf(__fsub_rn(box.x, ghix), __fsub_rn(glox, box.z));
+    const float sy = fmaxf(__fsub_rn(box.y, ghiy), __fsub_rn(gloy, box.w));
+    return __fmul_rn(L, L) < __fmul_rn(th2, d2) && (sx > 0.0f || sy > 0.0f);
+}
+
 // Group-walk stack and list capacities (per warp).
 constexpr int kGroupStack = 1024;
 constexpr int kGroupDfsAt = kGroupStack - 128;  // switch to one node per step above this depth

@@ -309,10 +309,6 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
                     const float4 m4 = __ldg(&gp->mom);
                     const float4 q4 = __ldg(&gp->quad);
                     const uint4 lk = __ldg(&gp->link);
-                    const float dx = fmaxf(0.0f, fmaxf(__fsub_rn(box.x, ghix), __fsub_rn(glox, box.z)));
-                    const float dy = fmaxf(0.0f, fmaxf(__fsub_rn(box.y, ghiy), __fsub_rn(gloy, box.w)));
-                    const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-                    const float L = fmaxf(__fsub_rn(box.z, box.x), __fsub_rn(box.w, box.y));
                     const uint32_t f = lk.z, e = lk.z + lk.w;
                     if (e <= sys_lo || f >= sys_hi) {
                         // another system's subtree: no interaction
@@ -320,7 +316,7 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
                         push = true;  // spans several systems: always open
                         r0 = lk.x;
                         r1 = lk.y;
-                    } else if (__fmul_rn(L, L) < __fmul_rn(th2, d2)) {
+                    } else if (group_accepts(box, m4.x, m4.y, glox, gloy, ghix, ghiy, th2)) {
                         emit_node = true;
                         mom = m4;
                         sq = q4;
