@@ -134,7 +134,13 @@ int bh_compute_accelerations(bh_sim* sim, float* acc_host);
  *   node_children[2(n-1)]: {left, right} per internal node
  *   node_parent[2n-1]: parent index, 0xFFFFFFFF at the root
  *   node_aabb[4(n-1)]: {min.x, min.y, max.x, max.y} per internal node
- *                      (a leaf's box is its body position) */
+ *                      (a leaf's box is its body position)
+ * With walk_mode BH_WALK_GROUP the step keeps the internal nodes in packed
+ * 64-byte records and writes the internal entries of node4, node_children
+ * and node_aabb only on request: each bh_get_buffers call (stream-ordered on
+ * the handle's stream) and each bh_read_buffer of those names refreshes them
+ * for the current tree.  Leaves, node_parent and the body arrays are
+ * current after every step in both modes. */
 typedef struct bh_buffers {
     float* mass;
     float* pos;

@@ -156,6 +156,7 @@ cudaError_t sort_init_attributes();
 int sort_passes(const DeviceBuffers& b);
 // tree.cu
 void launch_build_fill(const DeviceBuffers& b, int fp64_levels, cudaStream_t s);
+void launch_ref_layout(const DeviceBuffers& b, cudaStream_t s);  // group walk: node4/aabb/children/range on request
 void init_bound(const DeviceBuffers& b, cudaStream_t s);
 // walk.cu
 void launch_walk(const DeviceBuffers& b, const WalkParams& p, int block, cudaStream_t s);

@@ -918,6 +918,9 @@ extern "C" int bh_get_buffers(bh_sim* s, bh_buffers* out) {
     BH_HANDLE(s);
     if (!out) return fail(s, BH_ERR_INVALID_ARGUMENT, "null output");
     const DeviceBuffers& b = s->b;
+    // Group walk: the reference-layout internal-node arrays are derived from
+    // the packed records on request (stream-ordered after the last step).
+    if (b.gnode) bh::launch_ref_layout(b, s->stream);
     out->mass = b.mass;
     out->pos = (float*)b.pos;
     out->vel = (float*)b.vel;
@@ -962,6 +965,8 @@ extern "C" int bh_read_buffer(bh_sim* s, const char* name, void* host, size_t by
     else if (nm == "node_aabb") { src = b.aabb; cap = 16 * ni; }
     else return fail(s, BH_ERR_INVALID_ARGUMENT, "unknown buffer name: " + nm);
     if (bytes > cap) return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_read_buffer: size above the buffer");
+    if (b.gnode && (nm == "node4" || nm == "node_children" || nm == "node_aabb"))
+        bh::launch_ref_layout(b, s->stream);
     BH_CUDA(s, cudaStreamSynchronize(s->stream));
     if (bytes) BH_CUDA(s, cudaMemcpy(host, src, bytes, cudaMemcpyDeviceToHost));
     return BH_OK;

@@ -52,7 +52,7 @@ __device__ __forceinline__ uint32_t block_excl_scan_256(uint32_t v, uint32_t* s_
 }
 
 template <typename K, bool FIRST>
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, 2)
 onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_in,
                 K* __restrict__ keys_out, uint32_t* __restrict__ ids_out, uint32_t n, int pass,
                 StepScratch* __restrict__ scratch, uint32_t* __restrict__ status, uint32_t tiles,

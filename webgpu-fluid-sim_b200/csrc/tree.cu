@@ -8,19 +8,57 @@ void init_bound(const DeviceBuffers& b, cudaStream_t s) {
     if (b.n > 1) cudaMemsetAsync(b.bound, 0xFF, sizeof(uint32_t) * (b.n - 1), s);
 }
 
+template <typename K>
+static void launch_typed(const DeviceBuffers& b, int fp64_levels, cudaStream_t s) {
+    BuildArgs<K> a;
+    a.keys = (const K*)b.codes;
+    a.ids = b.ids;
+    a.mass = b.mass;
+    a.pos = b.pos;
+    a.node4 = b.node4;
+    a.children = b.children;
+    a.parent = b.parent;
+    a.aabb = b.aabb;
+    a.range = b.range;
+    a.big = b.big;
+    a.bound = b.bound;
+    a.n = b.n;
+    a.fp64 = fp64_levels;
+    a.gnode = b.gnode;
+    a.groups = b.groups;
+    a.group_count = b.groups ? &b.scratch->group_ctr[1] : nullptr;
+    a.gmax = b.group_max;
+    build_fill_kernel<K><<<(b.n + 255) / 256, 256, 0, s>>>(a);
+}
+
+// Reference-layout internal-node arrays from the packed records: node4
+// {com, mass, length}, aabb, children {left, right} and the slot range.
+static __global__ void __launch_bounds__(256)
+ref_layout_kernel(const GNode* __restrict__ gnode, uint32_t ni, float4* __restrict__ node4,
+                  float4* __restrict__ aabb, uint2* __restrict__ children, uint2* __restrict__ range) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < ni; v += gridDim.x * blockDim.x) {
+        const float4 box = __ldg(&gnode[v].box);
+        const float4 mom = __ldg(&gnode[v].mom);
+        const uint4 lk = __ldg(&gnode[v].link);
+        node4[v] = mom;
+        aabb[v] = box;
+        children[v] = make_uint2(lk.x, lk.y);
+        range[v] = make_uint2(lk.z, lk.z + lk.w - 1u);
+    }
+}
+
+void launch_ref_layout(const DeviceBuffers& b, cudaStream_t s) {
+    if (!b.gnode || b.n < 2) return;
+    const uint32_t ni = b.n - 1;
+    int blocks = (int)((ni + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    ref_layout_kernel<<<blocks, 256, 0, s>>>(b.gnode, ni, b.node4, b.aabb, b.children, b.range);
+}
+
 void launch_build_fill(const DeviceBuffers& b, int fp64_levels, cudaStream_t s) {
     if (b.n == 0) return;
-    const int blocks = (int)((b.n + 255) / 256);
-    if (b.key_bytes == 8)
-        build_fill_kernel<uint64_t><<<blocks, 256, 0, s>>>(
-            (const uint64_t*)b.codes, b.ids, b.mass, b.pos, b.node4, b.children, b.parent, b.aabb,
-            b.range, b.big, b.bound, b.n, fp64_levels, b.gnode, b.groups,
-            b.groups ? &b.scratch->group_ctr[1] : nullptr, b.group_max);
-    else
-        build_fill_kernel<uint32_t><<<blocks, 256, 0, s>>>(
-            (const uint32_t*)b.codes, b.ids, b.mass, b.pos, b.node4, b.children, b.parent, b.aabb,
-            b.range, b.big, b.bound, b.n, fp64_levels, b.gnode, b.groups,
-            b.groups ? &b.scratch->group_ctr[1] : nullptr, b.group_max);
+    if (b.key_bytes == 8) launch_typed<uint64_t>(b, fp64_levels, s);
+    else launch_typed<uint32_t>(b, fp64_levels, s);
 }
 
 }  // namespace bh

@@ -65,6 +65,32 @@ static cudaError_t scratch_address(unsigned char** out) {
     return cudaSuccess;
 }
 
+template <typename K>
+static void launch_static(const void* codes, const uint32_t* ids, const float* mass,
+                          const float* pos, uint32_t n, float* node4, uint32_t* children,
+                          uint32_t* parent, float* aabb, uint2* range, double2* big,
+                          uint32_t* bound, int fp64, cudaStream_t s) {
+    BuildArgs<K> a;
+    a.keys = static_cast<const K*>(codes);
+    a.ids = ids;
+    a.mass = mass;
+    a.pos = reinterpret_cast<const float2*>(pos);
+    a.node4 = reinterpret_cast<float4*>(node4);
+    a.children = reinterpret_cast<uint2*>(children);
+    a.parent = parent;
+    a.aabb = reinterpret_cast<float4*>(aabb);
+    a.range = range;
+    a.big = big;
+    a.bound = bound;
+    a.n = n;
+    a.fp64 = fp64;
+    a.gnode = nullptr;
+    a.groups = nullptr;
+    a.group_count = nullptr;
+    a.gmax = 0u;
+    build_fill_kernel<K><<<(n + 255) / 256, 256, 0, s>>>(a);
+}
+
 }  // namespace bh
 
 static int static_fail(int code, const std::string& msg) {
@@ -106,19 +132,12 @@ extern "C" int bh_build_hierarchy_static(const void* sorted_codes, int32_t morto
             return static_fail(BH_ERR_CUDA, std::string("cudaMemsetAsync(static exchange slots): ") +
                                                 cudaGetErrorString(e));
     }
-    const int blocks = (int)((n + 255) / 256);
-    float4* n4 = reinterpret_cast<float4*>(node4);
-    uint2* ch = reinterpret_cast<uint2*>(node_children);
-    float4* bx = reinterpret_cast<float4*>(node_aabb);
-    const float2* p2 = reinterpret_cast<const float2*>(pos);
     if (morton_bits == 64)
-        build_fill_kernel<uint64_t><<<blocks, 256, 0, s>>>(
-            static_cast<const uint64_t*>(sorted_codes), sorted_ids, mass, p2, n4, ch, node_parent,
-            bx, range, big, bound, n, fp64_levels, nullptr, nullptr, nullptr, 0u);
+        launch_static<uint64_t>(sorted_codes, sorted_ids, mass, pos, n, node4, node_children,
+                                node_parent, node_aabb, range, big, bound, fp64_levels, s);
     else
-        build_fill_kernel<uint32_t><<<blocks, 256, 0, s>>>(
-            static_cast<const uint32_t*>(sorted_codes), sorted_ids, mass, p2, n4, ch, node_parent,
-            bx, range, big, bound, n, fp64_levels, nullptr, nullptr, nullptr, 0u);
+        launch_static<uint32_t>(sorted_codes, sorted_ids, mass, pos, n, node4, node_children,
+                                node_parent, node_aabb, range, big, bound, fp64_levels, s);
     e = cudaGetLastError();
     if (e != cudaSuccess)
         return static_fail(BH_ERR_CUDA, std::string("build_fill_kernel launch: ") + cudaGetErrorString(e));
