@@ -41,10 +41,54 @@ struct VjpSmem {
     float4 body[32];           // staged leaf records {x, y, m, slot bits}
 };
 
-__device__ __forceinline__ float warp_sum(float v) {
+// Warp sums of 8 values by recursive halving: 4 + 2 + 1 exchanges split the
+// values between lane halves, 2 more finish the sum.  Afterwards lanes 4k..4k+3
+// hold the sum of v[k] (9 shuffles instead of 8 x 5).
+__device__ __forceinline__ float warp_reduce_scatter8(float v[8]) {
+    const unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const bool h4 = lane & 16, h3 = lane & 8, h2 = lane & 4;
+    float a[4], b[2];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-    return v;
+    for (int j = 0; j < 4; ++j) {
+        const float keep = h4 ? v[j + 4] : v[j], send = h4 ? v[j] : v[j + 4];
+        a[j] = keep + __shfl_xor_sync(FULL, send, 16);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const float keep = h3 ? a[j + 2] : a[j], send = h3 ? a[j] : a[j + 2];
+        b[j] = keep + __shfl_xor_sync(FULL, send, 8);
+    }
+    float c;
+    {
+        const float keep = h2 ? b[1] : b[0], send = h2 ? b[0] : b[1];
+        c = keep + __shfl_xor_sync(FULL, send, 4);
+    }
+    c += __shfl_xor_sync(FULL, c, 2);
+    c += __shfl_xor_sync(FULL, c, 1);
+    return c;
+}
+
+// Same for 4 values: lanes 8k..8k+7 hold the sum of v[k] (6 shuffles).
+__device__ __forceinline__ float warp_reduce_scatter4(float v[4]) {
+    const unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const bool h4 = lane & 16, h3 = lane & 8;
+    float a[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const float keep = h4 ? v[j + 2] : v[j], send = h4 ? v[j] : v[j + 2];
+        a[j] = keep + __shfl_xor_sync(FULL, send, 16);
+    }
+    float c;
+    {
+        const float keep = h3 ? a[1] : a[0], send = h3 ? a[0] : a[1];
+        c = keep + __shfl_xor_sync(FULL, send, 8);
+    }
+    c += __shfl_xor_sync(FULL, c, 4);
+    c += __shfl_xor_sync(FULL, c, 2);
+    c += __shfl_xor_sync(FULL, c, 1);
+    return c;
 }
 
 // node_adj: 6 floats per internal node {cbar.x, cbar.y, mbar, Q'bar xx, xy, yy}
@@ -134,24 +178,16 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
                     cbx += rbx;
                     cby += rby;
                 }
-                cbx = warp_sum(cbx);
-                cby = warp_sum(cby);
-                mb = warp_sum(mb);
                 if (MP >= 2) {
-                    gxx = warp_sum(gxx);
-                    gxy = warp_sum(gxy);
-                    gyy = warp_sum(gyy);
-                }
-                if (lane == 0) {
-                    float* na = node_adj + 6 * (size_t)v;
-                    atomicAdd(na + 0, cbx);
-                    atomicAdd(na + 1, cby);
-                    atomicAdd(na + 2, mb);
-                    if (MP >= 2) {
-                        atomicAdd(na + 3, gxx);
-                        atomicAdd(na + 4, gxy);
-                        atomicAdd(na + 5, gyy);
-                    }
+                    float vals[8] = {cbx, cby, mb, gxx, gxy, gyy, 0.f, 0.f};
+                    const float tot = warp_reduce_scatter8(vals);
+                    const int q = lane >> 2;  // lanes 4q hold the sum of vals[q]
+                    if ((lane & 3) == 0 && q < 6) atomicAdd(node_adj + 6 * (size_t)v + q, tot);
+                } else {
+                    float vals[4] = {cbx, cby, mb, 0.f};
+                    const float tot = warp_reduce_scatter4(vals);
+                    const int q = lane >> 3;  // lanes 8q hold the sum of vals[q]
+                    if ((lane & 7) == 0 && q < 3) atomicAdd(node_adj + 6 * (size_t)v + q, tot);
                 }
             }
         };
@@ -185,13 +221,12 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
                     cby += rby;
                     mb += ar * s3;
                 }
-                cbx = warp_sum(cbx);
-                cby = warp_sum(cby);
-                mb = warp_sum(mb);
-                if (lane == 0) {
-                    atomicAdd(&xbar_slot[sj].x, cbx);
-                    atomicAdd(&xbar_slot[sj].y, cby);
-                    atomicAdd(&mbar_slot[sj], mb);
+                {
+                    float vals[4] = {cbx, cby, mb, 0.f};
+                    const float tot = warp_reduce_scatter4(vals);
+                    const int q = lane >> 3;  // lanes 8q hold the sum of vals[q]
+                    if ((lane & 7) == 0 && q < 3)
+                        atomicAdd(q == 2 ? &mbar_slot[sj] : (q == 0 ? &xbar_slot[sj].x : &xbar_slot[sj].y), tot);
                 }
             }
         };

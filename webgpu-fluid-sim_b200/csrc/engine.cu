@@ -55,6 +55,12 @@ struct bh_sim {
                *seg_pos = nullptr, *fin_pos = nullptr, *fin_vel = nullptr;
         float *mbar_slot = nullptr, *mbar = nullptr;
         double* loss = nullptr;
+        // Trees of one replayed segment, one record per step (null when the
+        // segment does not fit the memory budget: the reverse sweep then
+        // rebuilds each tree).
+        void* slab = nullptr;
+        size_t slab_stride = 0;
+        uint32_t slab_steps = 0;
     } adj;
     // ensemble of independent systems (empty: one system)
     std::vector<uint32_t> sys_sizes;
@@ -152,7 +158,60 @@ static void destroy_graphs(bh_sim* s) {
 
 static void free_adjoint(bh_sim* s) {
     if (s->adj.arena) cudaFree(s->adj.arena);
+    if (s->adj.slab) cudaFree(s->adj.slab);
     s->adj = bh_sim::Adjoint();
+}
+
+// Per-step record of the slab: what the force VJP reads of a tree.
+struct TreeRecord {
+    size_t gnode, node4, groups, ids, parent, ctr, bytes;
+};
+
+static TreeRecord tree_record(uint32_t n) {
+    const size_t nn = n ? 2 * (size_t)n - 1 : 1, ni = n > 1 ? (size_t)n - 1 : 1, nb = n ? n : 1;
+    auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    TreeRecord r;
+    r.gnode = 0;
+    r.node4 = up(r.gnode + sizeof(bh::GNode) * ni);  // full node4 extent; only the leaves are copied
+    r.groups = up(r.node4 + sizeof(float4) * nn);
+    r.ids = up(r.groups + sizeof(uint2) * nb);
+    r.parent = up(r.ids + sizeof(uint32_t) * nb);
+    r.ctr = up(r.parent + sizeof(uint32_t) * nn);
+    r.bytes = up(r.ctr + 4 * sizeof(unsigned int));
+    return r;
+}
+
+// Device buffers whose tree (and walk work counters) come from slab record k.
+static DeviceBuffers slab_view(bh_sim* s, uint32_t k) {
+    const TreeRecord r = tree_record(s->b.n);
+    char* base = (char*)s->adj.slab + (size_t)k * s->adj.slab_stride;
+    DeviceBuffers bb = s->b;
+    bb.gnode = (bh::GNode*)(base + r.gnode);
+    bb.node4 = (float4*)(base + r.node4);
+    bb.groups = (uint2*)(base + r.groups);
+    bb.ids = (uint32_t*)(base + r.ids);
+    bb.parent = (uint32_t*)(base + r.parent);
+    return bb;
+}
+
+// Save the tree just built by a step into slab record k.
+static int save_tree(bh_sim* s, uint32_t k) {
+    const uint32_t n = s->b.n;
+    const TreeRecord r = tree_record(n);
+    char* base = (char*)s->adj.slab + (size_t)k * s->adj.slab_stride;
+    const DeviceBuffers& b = s->b;
+    cudaStream_t st = s->stream;
+    const size_t nm1 = n - 1;
+    if (n > 1) BH_CUDA(s, cudaMemcpyAsync(base + r.gnode, b.gnode, sizeof(bh::GNode) * nm1, cudaMemcpyDeviceToDevice, st));
+    BH_CUDA(s, cudaMemcpyAsync(base + r.node4 + sizeof(float4) * nm1, b.node4 + nm1, sizeof(float4) * (size_t)n,
+                               cudaMemcpyDeviceToDevice, st));
+    BH_CUDA(s, cudaMemcpyAsync(base + r.groups, b.groups, sizeof(uint2) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    BH_CUDA(s, cudaMemcpyAsync(base + r.ids, b.ids, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    BH_CUDA(s, cudaMemcpyAsync(base + r.parent, b.parent, sizeof(uint32_t) * (2 * (size_t)n - 1),
+                               cudaMemcpyDeviceToDevice, st));
+    BH_CUDA(s, cudaMemcpyAsync(base + r.ctr, b.scratch->group_ctr, 4 * sizeof(unsigned int),
+                               cudaMemcpyDeviceToDevice, st));
+    return BH_OK;
 }
 
 static void free_buffers(bh_sim* s) {
@@ -787,6 +846,26 @@ static int ensure_adjoint(bh_sim* s, uint32_t nck, uint32_t seg) {
     a.fin_pos = (float2*)(p + o_fp);
     a.fin_vel = (float2*)(p + o_fv);
     a.loss = (double*)(p + o_ls);
+    // Replayed trees for the reverse sweep: one record per step of a segment,
+    // within 4 GB and a quarter of the free device memory.
+    const TreeRecord r = tree_record(n);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        free_b = 0;
+    }
+    const size_t want = r.bytes * (size_t)seg;
+    const size_t budget = free_b / 4 < ((size_t)4 << 30) ? free_b / 4 : ((size_t)4 << 30);
+    if (n > 1 && s->cfg.walk_mode == BH_WALK_GROUP && want <= budget) {
+        void* slab = nullptr;
+        if (cudaMalloc(&slab, want) == cudaSuccess) {
+            a.slab = slab;
+            a.slab_stride = r.bytes;
+            a.slab_steps = seg;
+        } else {
+            cudaGetLastError();  // fall back to rebuilding each tree
+        }
+    }
     return BH_OK;
 }
 
@@ -797,6 +876,18 @@ static void enqueue_force_vjp(bh_sim* s, const float2* at, const float2* abar) {
     enqueue_tree_on(s, bb, [](int) {});
     bh::launch_force_vjp(bb, walk_params(s, bh::kWalkForces), abar, s->adj.node_adj,
                          s->adj.xbar_slot, s->adj.mbar_slot, s->adj.xbar, s->adj.mbar, s->stream);
+}
+
+// Same, on the tree saved in slab record k (built at those positions).
+static void enqueue_force_vjp_saved(bh_sim* s, uint32_t k, const float2* abar) {
+    DeviceBuffers bb = slab_view(s, k);
+    const TreeRecord r = tree_record(s->b.n);
+    unsigned int* ctr = (unsigned int*)((char*)s->adj.slab + (size_t)k * s->adj.slab_stride + r.ctr);
+    cudaMemsetAsync(ctr, 0, sizeof(unsigned int), s->stream);  // work counter; [1] = group count
+    bh::WalkParams p = walk_params(s, bh::kWalkForces);
+    p.group_ctr = ctr;
+    bh::launch_force_vjp(bb, p, abar, s->adj.node_adj, s->adj.xbar_slot, s->adj.mbar_slot,
+                         s->adj.xbar, s->adj.mbar, s->stream);
 }
 
 extern "C" int bh_force_vjp(bh_sim* s, const float* abar, float* xbar, float* mbar) {
@@ -858,16 +949,20 @@ extern "C" int bh_rollout_grad(bh_sim* s, uint32_t steps, uint32_t checkpoint_ev
         BH_CUDA(s, cudaMemcpyAsync(s->b.vel, a.ck_vel + (size_t)seg * n, vb, cudaMemcpyDeviceToDevice, st));
         s->acc_valid = false;
         BH_CUDA(s, cudaMemcpyAsync(a.seg_pos, s->b.pos, vb, cudaMemcpyDeviceToDevice, st));
+        const bool saved = a.slab && a.slab_steps >= e - c;
         for (uint32_t k = c; k < e; ++k) {
             if ((rc = step_once(s)) != BH_OK) return rc;
             BH_CUDA(s, cudaMemcpyAsync(a.seg_pos + (size_t)(k + 1 - c) * n, s->b.pos, vb,
                                        cudaMemcpyDeviceToDevice, st));
+            // the step's tree is the one at x_{k+1}, where its reverse step needs the VJP
+            if (saved && (rc = save_tree(s, k - c)) != BH_OK) return rc;
         }
         for (int64_t k = (int64_t)e - 1; k >= (int64_t)c; --k) {
             // closing kick of step k (force at x_{k+1}) plus the pending opening
             // kick of step k+1 at the same point
             bh::launch_adj_pre(a.apend, a.vbar, h, n, a.abar, st);
-            enqueue_force_vjp(s, a.seg_pos + (size_t)(k + 1 - c) * n, a.abar);
+            if (saved) enqueue_force_vjp_saved(s, (uint32_t)(k - c), a.abar);
+            else enqueue_force_vjp(s, a.seg_pos + (size_t)(k + 1 - c) * n, a.abar);
             // drift, then the opening kick of step k (force at x_k, pending)
             bh::launch_adj_post(a.xbar, a.vbar, a.apend, dt, h, n, st);
         }
