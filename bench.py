@@ -44,6 +44,10 @@ sys.path.insert(0, ROOT)
 PKG = "webgpu-fluid-sim_b200"
 DEFAULT_WORKLOAD = "colliding-disks-800k"
 FLUSH_BYTES = 256 << 20  # > 126 MB L2
+# DRAM bytes (read + write) of one launch of the dominant kernel (the walk),
+# from one ncu capture of the same workload
+# (profiles/walk_group_build_fill_onesweep_colliding-disks-800k.md).
+NCU_WALK_TRAFFIC_BYTES = {"colliding-disks-800k": 53.05e6}
 
 
 def parse():
@@ -505,7 +509,9 @@ def run_own(args):
         fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # nominal FMA peak at max clock
         achieved = flops / (walk_ms / 1e3) / 1e12
         roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                    "frac": achieved / fp32_peak, "traffic": None,
+                    "frac": achieved / fp32_peak,
+                    "traffic": NCU_WALK_TRAFFIC_BYTES.get(args.workload),
+                    "traffic_unit": "bytes per launch (ncu dram read + write)",
                     "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2 x max SM clock);"
                                    " no measured FP32 peak exists for this pool",
                     "kernel": "walk", "kernel_ms": walk_ms,
