@@ -145,6 +145,40 @@ def test_large_tree_properties_800k(bh):
     sim.close()
 
 
+@pytest.mark.parametrize("cfg", [
+    dict(walk="group", mortonBits=64, softening="plummer", plummerEps=1e-4, bhTheta=0.5),
+    dict(mortonDomain="bbox", softening="plummer", bhTheta=0.5),
+], ids=["group-64bit", "reference-layout-32bit"])
+def test_split_build_matches_oracle_beyond_2m(bh, orc, cfg):
+    # From 2^21 bodies the build runs as a block-local kernel plus a climb of
+    # the frontier nodes it leaves; both node layouts against the oracle.
+    n = (1 << 21) + 4097
+    sim = make_sim(bh, n, "gaussian-mixture", seed=3, **cfg)
+    # bbox, encode, sort passes, build (2 kernels), walk
+    assert sim.kernels_per_step() == (1 + 1 + 8 + 2 + 1 if cfg.get("mortonBits") == 64
+                                      else 1 + 1 + 4 + 2 + 1)
+    mass, pos, vel = sim.download()
+    sim.computeAccelerations()
+    t = sim.tree()
+    p = orc.params_from_config(sim.config)
+    codes, ids = orc.morton(p, pos)
+    codes, ids = orc.sort(codes, ids)
+    left, right, parent = orc.build(codes, sim.config.mortonBits)
+    com, mnode, aabb, length = orc.fill(ids, mass, pos, left, right, parent)
+    assert (t["codes"].astype(np.uint64) == codes).all(), "Morton codes differ"
+    assert (t["ids"] == ids).all(), "sorted permutation differs"
+    assert (t["parent"] == parent).all(), "parent array differs"
+    assert (t["children"][:, 0] == left[: n - 1]).all(), "left children differ"
+    assert (t["children"][:, 1] == right[: n - 1]).all(), "right children differ"
+    assert (t["aabb"] == aabb[: n - 1]).all(), "AABBs differ"
+    assert (t["node4"][:, 3] == length).all(), "lengths differ"
+    m_gpu = t["node4"][:, 2]
+    assert np.all(np.abs(m_gpu - mnode) <= 1e-5 * np.abs(mnode) + 1e-30)
+    scale = np.abs(com).max(1) + length
+    assert np.all(np.abs(t["node4"][:, :2] - com).max(1) <= 1e-5 * scale + 1e-30)
+    sim.close()
+
+
 def test_graph_and_direct_paths_agree(bh):
     outs = []
     for graphs in (True, False):

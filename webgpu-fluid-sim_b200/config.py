@@ -88,4 +88,11 @@ WORKLOADS = {
                                                plummerEps=1e-4, mortonBits=64,
                                                integrator="leapfrog-kdk", walk="group",
                                                leafSize=8)),
+    # N=4,194,304 from the same Gaussian-mixture generator and settings: the
+    # profiling case of the 16M point (inputs > L2, a few GB on the device)
+    "gaussian-mixture-4m": dict(n=4_194_304, scenario="gaussian-mixture", steps=50,
+                                config=Config(bhTheta=0.5, deltaTime=1e-5, softening="plummer",
+                                              plummerEps=1e-4, mortonBits=64,
+                                              integrator="leapfrog-kdk", walk="group",
+                                              leafSize=8)),
 }

@@ -17,10 +17,16 @@ constexpr int kStackSize = 256;  // barnes_hut.wgsl:67
 // Nodes with at least this many bodies aggregate mass/COM in FP64.
 constexpr uint32_t kFp64MinBodies = 1024;
 
-// Sort tiling.
-constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+// Sort tiling (a tile is kSortThreads x kSortItems keys).
+#ifndef BH_SORT_THREADS
+#define BH_SORT_THREADS 512
+#endif
+#ifndef BH_SORT_ITEMS
+#define BH_SORT_ITEMS 12
+#endif
+constexpr int kSortThreads = BH_SORT_THREADS;
+constexpr int kSortItems = BH_SORT_ITEMS;
+constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 256;
 
@@ -99,6 +105,7 @@ struct StepScratch {
     uint32_t bbox[4];          // ordered-int max of {-minx, -miny, maxx, maxy} (see morton.cu)
     unsigned long long walk_counts[4];  // instrumented walk counters
     unsigned int group_ctr[4];          // group walk: [0] work counter, [1] number of groups
+    unsigned int frontier_ctr;          // hierarchy build: frontier nodes of the local phase
 };
 
 struct DeviceBuffers {
@@ -127,6 +134,7 @@ struct DeviceBuffers {
     GNode* gnode = nullptr;      // n-1 packed records (group walk only; else null)
     uint2* groups = nullptr;     // n {first slot, count}: maximal subtrees of <= G bodies (group walk)
     uint32_t group_max = 0;      // G = 32 x bodies per lane (0: no groups)
+    uint2* frontier = nullptr;   // n {first slot, last slot}: nodes left by the build's local phase
     // scratch
     StepScratch* scratch = nullptr;
     uint32_t* status = nullptr;  // look-back status: passes * tiles * 256
@@ -156,6 +164,9 @@ cudaError_t sort_init_attributes();
 int sort_passes(const DeviceBuffers& b);
 // tree.cu
 void launch_build_fill(const DeviceBuffers& b, int fp64_levels, cudaStream_t s);
+// Bodies from which the build runs as two kernels (local phase + frontier climb).
+constexpr uint32_t kSplitBuildMin = 1u << 21;
+bool split_build(uint32_t n);
 void launch_ref_layout(const DeviceBuffers& b, cudaStream_t s);  // group walk: node4/aabb/children/range on request
 void init_bound(const DeviceBuffers& b, cudaStream_t s);
 // walk.cu

@@ -248,6 +248,7 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     size_t o_node4 = c.take<float4>(nn), o_child = c.take<uint2>(ni), o_parent = c.take<uint32_t>(nn);
     size_t o_aabb = c.take<float4>(ni), o_range = c.take<uint2>(ni), o_big = c.take<double2>(2 * ni);
     size_t o_bound = c.take<uint32_t>(ni);
+    size_t o_front = c.take<uint2>(nb);
     const bool group = s->cfg.walk_mode == BH_WALK_GROUP;
     size_t o_gnode = group ? c.take<bh::GNode>(ni) : 0;
     size_t o_groups = group ? c.take<uint2>(nb) : 0;
@@ -285,6 +286,7 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     b.range = (uint2*)(a + o_range);
     b.big = (double2*)(a + o_big);
     b.bound = (uint32_t*)(a + o_bound);
+    b.frontier = (uint2*)(a + o_front);
     b.gnode = group ? (bh::GNode*)(a + o_gnode) : nullptr;
     b.groups = group ? (uint2*)(a + o_groups) : nullptr;
     b.group_max = group ? 32u * (uint32_t)(s->cfg.bodies_per_lane > 0 ? s->cfg.bodies_per_lane : 2) : 0u;
@@ -1179,7 +1181,7 @@ extern "C" int bh_kernels_per_step(bh_sim* s, uint32_t* out) {
     if (needs_bbox(s) || s->b.num_systems) k += 1;                 // bbox (per system)
     k += 1;                                                         // encode
     k += (uint32_t)bh::sort_passes(s->b);                          // sort passes
-    k += 1;                                                         // build + fill
+    k += bh::split_build(s->b.n) ? 2 : 1;                           // build + fill (+ frontier climb)
     k += 1;                                                         // walk + integrate
     *out = s->b.n ? k : 0;
     return BH_OK;

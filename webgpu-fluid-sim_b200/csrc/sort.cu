@@ -9,7 +9,7 @@
 // Design (onesweep, one kernel per 8-bit digit):
 //  - The digit histograms of every pass come from the encode kernel, so each
 //    pass reads its keys exactly once.
-//  - A CTA takes the next 4096-key tile from an atomic counter (so lower
+//  - A CTA takes the next tile (kSortTile keys) from an atomic counter (so lower
 //    tiles are always already running), ranks its keys warp by warp with
 //    __match_any_sync (stable: item-major, lane-minor = memory order),
 //    publishes its per-digit counts, and resolves its global offsets by a
@@ -33,7 +33,9 @@ constexpr uint32_t kFlagMask = 3u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1;
 constexpr uint32_t kSpinCap = 1u << 22;
 
-__device__ __forceinline__ uint32_t block_excl_scan_256(uint32_t v, uint32_t* s_tot) {
+// Exclusive scan over the block (every thread takes part; threads past the
+// 256 digits pass 0, so the digits' prefixes are unaffected by them).
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_tot) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t x = v;
 #pragma unroll
@@ -45,14 +47,18 @@ __device__ __forceinline__ uint32_t block_excl_scan_256(uint32_t v, uint32_t* s_
     __syncthreads();
     uint32_t before = 0;
 #pragma unroll
-    for (int w = 0; w < kSortThreads / 32; ++w)
+    for (int w = 0; w < kRadix / 32; ++w)
         if (w < warp) before += s_tot[w];
     __syncthreads();
     return before + x - v;
 }
 
+#ifndef BH_SORT_MIN_BLOCKS
+#define BH_SORT_MIN_BLOCKS 2
+#endif
+
 template <typename K, bool FIRST>
-__global__ void __launch_bounds__(kSortThreads, 2)
+__global__ void __launch_bounds__(kSortThreads, BH_SORT_MIN_BLOCKS)
 onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_in,
                 K* __restrict__ keys_out, uint32_t* __restrict__ ids_out, uint32_t n, int pass,
                 StepScratch* __restrict__ scratch, uint32_t* __restrict__ status, uint32_t tiles,
@@ -109,27 +115,31 @@ onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_
         __syncwarp();
     }
     __syncthreads();
-    // Per digit: exclusive prefix over warps, and the tile's count.
-    const uint32_t d = (uint32_t)tid;
+    // Per digit (threads 0..255): exclusive prefix over warps, and the tile's count.
+    static_assert(kSortThreads >= kRadix && kSortThreads % 32 == 0, "one thread per digit");
+    const bool digit_thread = tid < kRadix;
+    const uint32_t d = digit_thread ? (uint32_t)tid : 0u;
     uint32_t run = 0;
+    if (digit_thread) {
 #pragma unroll
-    for (int w = 0; w < W; ++w) {
-        uint32_t c = s_whist[w][d];
-        s_whist[w][d] = run;
-        run += c;
+        for (int w = 0; w < W; ++w) {
+            uint32_t c = s_whist[w][d];
+            s_whist[w][d] = run;
+            run += c;
+        }
     }
     const uint32_t tile_cnt = run;
     // Publish this tile's aggregate (or inclusive prefix for tile 0).
     uint32_t* my_status = status + ((size_t)pass * tiles + tile) * kRadix;
-    {
+    if (digit_thread) {
         cuda::atomic_ref<uint32_t, cuda::thread_scope_device> a(my_status[d]);
         a.store((tile == 0 ? kFlagPrefix : kFlagAggregate) | tile_cnt, cuda::memory_order_relaxed);
     }
-    const uint32_t tile_excl = block_excl_scan_256(tile_cnt, s_tot);
-    const uint32_t glob_excl = block_excl_scan_256(scratch->hist[pass][d], s_tot);
+    const uint32_t tile_excl = block_excl_scan(tile_cnt, s_tot);
+    const uint32_t glob_excl = block_excl_scan(digit_thread ? scratch->hist[pass][d] : 0u, s_tot);
     // Decoupled look-back over earlier tiles, one digit per thread.
     uint32_t excl = 0;
-    if (tile > 0) {
+    if (tile > 0 && digit_thread) {
         int t = (int)tile - 1;
         uint32_t spins = 0;
         while (true) {
@@ -151,8 +161,10 @@ onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_
         cuda::atomic_ref<uint32_t, cuda::thread_scope_device> a(my_status[d]);
         a.store(kFlagPrefix | (excl + tile_cnt), cuda::memory_order_relaxed);
     }
-    s_tile_excl[d] = tile_excl;
-    s_gbase[d] = glob_excl + excl;
+    if (digit_thread) {
+        s_tile_excl[d] = tile_excl;
+        s_gbase[d] = glob_excl + excl;
+    }
     __syncthreads();
     // Stage in digit order.
 #pragma unroll

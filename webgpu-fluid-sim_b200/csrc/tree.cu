@@ -1,8 +1,12 @@
-// tree.cu -- launches the fused hierarchy build + fill for the engine's step.
-// The kernel and its derivation are in tree_kernel.cuh.
+// tree.cu -- launches the hierarchy build + fill for the engine's step: the
+// block-local phase (build_fill_kernel<K, true>) and the climb of the
+// frontier nodes it leaves (build_climb_kernel).  The kernels and their
+// derivation are in tree_kernel.cuh.
 #include "tree_kernel.cuh"
 
 namespace bh {
+
+bool split_build(uint32_t n) { return n >= kSplitBuildMin; }
 
 void init_bound(const DeviceBuffers& b, cudaStream_t s) {
     if (b.n > 1) cudaMemsetAsync(b.bound, 0xFF, sizeof(uint32_t) * (b.n - 1), s);
@@ -28,7 +32,29 @@ static void launch_typed(const DeviceBuffers& b, int fp64_levels, cudaStream_t s
     a.groups = b.groups;
     a.group_count = b.groups ? &b.scratch->group_ctr[1] : nullptr;
     a.gmax = b.group_max;
-    build_fill_kernel<K><<<(b.n + 255) / 256, 256, 0, s>>>(a);
+    const uint32_t grid = (b.n + kBuildBlock - 1) / kBuildBlock;
+    if (!split_build(b.n)) {
+        build_fill_kernel<K, false><<<grid, kBuildBlock, 0, s>>>(a);
+        return;
+    }
+    a.frontier = b.frontier;
+    a.frontier_count = &b.scratch->frontier_ctr;
+    build_fill_kernel<K, true><<<grid, kBuildBlock, 0, s>>>(a);
+    // Frontier nodes number far fewer than bodies (a handful per CTA), but
+    // only the device knows how many: a resident grid strides over them.
+    static int blocks_per_sm[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& bps = blocks_per_sm[dev & 63];
+    if (bps == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, build_climb_kernel<K>, kBuildBlock, 0);
+        if (bps < 1) bps = 1;
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    uint32_t blocks = (uint32_t)(sms * bps);
+    if (blocks > grid) blocks = grid;
+    build_climb_kernel<K><<<blocks, kBuildBlock, 0, s>>>(a);
 }
 
 // Reference-layout internal-node arrays from the packed records: node4

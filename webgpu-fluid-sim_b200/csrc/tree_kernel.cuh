@@ -89,6 +89,10 @@ struct BuildArgs {
     uint2* groups;
     unsigned int* group_count;
     uint32_t gmax;
+    // Split build only: nodes whose parent split is not local, as {first
+    // slot, last slot}, and their count (zero before the local phase).
+    uint2* frontier = nullptr;
+    unsigned int* frontier_count = nullptr;
 };
 
 // One thread per sorted slot climbs from its leaf; the lanes of a warp start
@@ -98,18 +102,263 @@ struct BuildArgs {
 constexpr int kBuildBlock = 256;
 static_assert(kFp64MinBodies > kBuildBlock, "local nodes must all take the f32 path");
 
+// The block-local shared state of the local phase.
 template <typename K>
+struct BuildShared {
+    K key[kBuildBlock + 2];           // keys of slots B0-1 .. B0+B
+    int d[kBuildBlock + 1];           // delta at boundary g = B0-1+q (between slots g, g+1)
+    int wmin[2][kBuildBlock / 32];    // per-warp minima for the two scans
+    int suf[kBuildBlock];             // suf[q] = min of d[q+1..B]
+    unsigned char local[kBuildBlock + 1];
+    uint32_t bound[kBuildBlock + 1];  // exchange slots of the local splits
+    float leaf[3][kBuildBlock];       // leaf {m, x, y} by slot - B0
+    float rec[10][kBuildBlock];       // local internal node {m, cx, cy, box, S} by index - B0
+};
+
+// The node a climbing thread currently owns: its slot range, the deltas at
+// the range's two boundaries, and its record.
+struct Climb {
+    uint32_t l, r;
+    int dl, dr;
+    float cm, cx, cy;
+    float lox, loy, hix, hiy;
+    float sxx, sxy, syy;       // second moments about the COM (group walk)
+    double dm, dmx, dmy;       // valid when the node has >= kFp64MinBodies bodies
+    bool local;                // still in the block-local phase
+};
+
+// One level of the climb from the node in `c`: returns false when this thread
+// is the first to arrive at the split (it stops; the sibling's thread goes
+// on) or has created the root, else true with `c` holding the parent.
+//   LOCAL: the thread starts in the block-local phase (shared memory `S` of
+//          the CTA owning slots [B0, B0 + kBuildBlock)).
+//   STOP:  at the first split that is not local, record the node in the
+//          frontier list and stop (the split build's first kernel); else go
+//          on with the device-scope protocol (fused build, second kernel).
+template <typename K, bool LOCAL, bool STOP>
+__device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, BuildShared<K>* S,
+                                           uint32_t B0) {
+    constexpr int B = kBuildBlock;
+    const uint32_t n = A.n, nm1 = n - 1;
+    bool local = LOCAL && c.local;
+    volatile float* vrec = LOCAL ? &S->rec[0][0] : nullptr;
+    volatile float* vleaf = LOCAL ? &S->leaf[0][0] : nullptr;
+    {
+        const bool is_left = c.dr > c.dl;
+        const uint32_t gamma = is_left ? c.r : c.l - 1;
+        int qg = 0;
+        if (LOCAL) {
+            qg = (int)((long long)gamma - ((long long)B0 - 1));
+            local = local && qg >= 1 && qg <= B - 1 && S->local[qg];
+            c.local = local;
+        }
+        if (STOP && !local) {
+            // The parent split lies outside this CTA: leave it to the climb kernel.
+            A.frontier[atomicAdd(A.frontier_count, 1u)] = make_uint2(c.l, c.r);
+            return false;
+        }
+        // Past the stop test a split build's first kernel is always local;
+        // its nodes hold fewer than kBuildBlock bodies, so never take FP64.
+        const bool IN_LOCAL = LOCAL && (STOP || local);
+        uint32_t other;
+        if (IN_LOCAL) {
+            // Shared-memory exchange: this node's record (in shared memory)
+            // is released to the CTA before the slot changes hands.
+            __threadfence_block();
+            other = atomicExch(&S->bound[qg], is_left ? c.l : c.r);
+            if (other == kSentinel) return false;
+            __threadfence_block();
+        } else {
+            // One acq_rel exchange releases this node's record and acquires
+            // the sibling's (release/acquire through bound[gamma]).
+            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> slot(A.bound[gamma]);
+            other = slot.exchange(is_left ? c.l : c.r, cuda::memory_order_acq_rel);
+            if (other == kSentinel) return false;  // first to arrive: the sibling finishes the parent
+            slot.store(kSentinel, cuda::memory_order_relaxed);
+        }
+        const uint32_t pl = is_left ? c.l : other;
+        const uint32_t pr = is_left ? other : c.r;
+        const uint32_t li = (pl == gamma) ? nm1 + gamma : gamma;
+        const uint32_t ri = (pr == gamma + 1) ? nm1 + gamma + 1 : gamma + 1;
+        const uint32_t sib = is_left ? ri : li;
+        const uint32_t sib_cnt = is_left ? (pr - gamma) : (gamma - pl + 1);
+        const uint32_t my_cnt = c.r - c.l + 1;
+        float4 s4, sb, sq = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (IN_LOCAL) {
+            // Sibling record from shared memory.
+            if (sib >= nm1) {
+                const int k = (int)(sib - nm1 - B0);
+                s4 = make_float4(vleaf[B + k], vleaf[2 * B + k], vleaf[k], 0.f);
+                sb = make_float4(s4.x, s4.y, s4.x, s4.y);
+            } else {
+                const int k = (int)(sib - B0);
+                s4 = make_float4(vrec[B + k], vrec[2 * B + k], vrec[k], 0.f);
+                sb = make_float4(vrec[3 * B + k], vrec[4 * B + k], vrec[5 * B + k], vrec[6 * B + k]);
+                sq = make_float4(vrec[7 * B + k], vrec[8 * B + k], vrec[9 * B + k], 0.f);
+            }
+        } else if (sib >= nm1) {
+            // Sibling record through L2 (written by another thread in this launch).
+            s4 = __ldcg(&A.node4[sib]);
+            sb = make_float4(s4.x, s4.y, s4.x, s4.y);
+        } else if (A.gnode) {
+            sb = __ldcg(&A.gnode[sib].box);
+            s4 = __ldcg(&A.gnode[sib].mom);
+            sq = __ldcg(&A.gnode[sib].quad);
+        } else {
+            s4 = __ldcg(&A.node4[sib]);
+            sb = __ldcg(&A.aabb[sib]);
+        }
+        c.lox = fminf(c.lox, sb.x);
+        c.loy = fminf(c.loy, sb.y);
+        c.hix = fmaxf(c.hix, sb.z);
+        c.hiy = fmaxf(c.hiy, sb.w);
+        const uint32_t cnt = pr - pl + 1;
+        // Parent's boundary deltas and its own Karras index.
+        int dpl, dpr;
+        if (is_left) {
+            dpl = c.dl;
+            dpr = (IN_LOCAL) ? S->d[(int)(pr - B0 + 1)]
+                                   : ((pr == nm1) ? -1 : delta_at(A.keys, pr, pr + 1));
+        } else {
+            dpr = c.dr;
+            dpl = (IN_LOCAL) ? S->d[(int)(pl - B0)]
+                                   : ((pl == 0) ? -1 : delta_at(A.keys, pl - 1, pl));
+        }
+        const uint32_t pidx = (pl == 0 && pr == nm1) ? 0u : ((dpr > dpl) ? pr : pl);
+        float tm, ncx, ncy;
+        if (!STOP && A.fp64 && cnt >= kFp64MinBodies) {
+            double sm, smx, smy;
+            if (sib_cnt >= kFp64MinBodies) {
+                const double2 s0 = __ldcg(&A.big[2 * (size_t)sib]);
+                const double2 s1 = __ldcg(&A.big[2 * (size_t)sib + 1]);
+                sm = s0.x; smx = s0.y; smy = s1.x;
+            } else {
+                sm = (double)s4.z; smx = (double)s4.z * (double)s4.x; smy = (double)s4.z * (double)s4.y;
+            }
+            if (my_cnt < kFp64MinBodies) {
+                c.dm = (double)c.cm; c.dmx = (double)c.cm * (double)c.cx; c.dmy = (double)c.cm * (double)c.cy;
+            }
+            c.dm += sm;
+            c.dmx += smx;
+            c.dmy += smy;
+            tm = (float)c.dm;
+            ncx = c.dm > 0.0 ? (float)(c.dmx / c.dm) : 0.0f;
+            ncy = c.dm > 0.0 ? (float)(c.dmy / c.dm) : 0.0f;
+            A.big[2 * (size_t)pidx] = make_double2(c.dm, c.dmx);
+            A.big[2 * (size_t)pidx + 1] = make_double2(c.dmy, 0.0);
+        } else {
+            float ml, mr, clx, cly, crx, cry;
+            if (is_left) { ml = c.cm; clx = c.cx; cly = c.cy; mr = s4.z; crx = s4.x; cry = s4.y; }
+            else { ml = s4.z; clx = s4.x; cly = s4.y; mr = c.cm; crx = c.cx; cry = c.cy; }
+            tm = __fadd_rn(ml, mr);
+            if (tm > 0.0f) {
+                ncx = __fdiv_rn(__fadd_rn(__fmul_rn(clx, ml), __fmul_rn(crx, mr)), tm);
+                ncy = __fdiv_rn(__fadd_rn(__fmul_rn(cly, ml), __fmul_rn(cry, mr)), tm);
+            } else {
+                ncx = 0.0f;
+                ncy = 0.0f;
+            }
+        }
+        const float len = fmaxf(__fsub_rn(c.hix, c.lox), __fsub_rn(c.hiy, c.loy));
+        if (A.gnode) {
+            // Second moments about the parent COM, left child first:
+            // S = sum_c S_c + m_c d_c d_c^T, d_c = c_c - c_parent (leaves: S_c = 0).
+            float ml, mr, lxx, lxy, lyy, rxx, rxy, ryy, dlx, dly, drx, dry;
+            if (is_left) {
+                ml = c.cm; lxx = c.sxx; lxy = c.sxy; lyy = c.syy; dlx = __fsub_rn(c.cx, ncx); dly = __fsub_rn(c.cy, ncy);
+                mr = s4.z; rxx = sq.x; rxy = sq.y; ryy = sq.z; drx = __fsub_rn(s4.x, ncx); dry = __fsub_rn(s4.y, ncy);
+            } else {
+                ml = s4.z; lxx = sq.x; lxy = sq.y; lyy = sq.z; dlx = __fsub_rn(s4.x, ncx); dly = __fsub_rn(s4.y, ncy);
+                mr = c.cm; rxx = c.sxx; rxy = c.sxy; ryy = c.syy; drx = __fsub_rn(c.cx, ncx); dry = __fsub_rn(c.cy, ncy);
+            }
+            c.sxx = __fadd_rn(__fadd_rn(lxx, __fmul_rn(ml, __fmul_rn(dlx, dlx))),
+                              __fadd_rn(rxx, __fmul_rn(mr, __fmul_rn(drx, drx))));
+            c.sxy = __fadd_rn(__fadd_rn(lxy, __fmul_rn(ml, __fmul_rn(dlx, dly))),
+                              __fadd_rn(rxy, __fmul_rn(mr, __fmul_rn(drx, dry))));
+            c.syy = __fadd_rn(__fadd_rn(lyy, __fmul_rn(ml, __fmul_rn(dly, dly))),
+                              __fadd_rn(ryy, __fmul_rn(mr, __fmul_rn(dry, dry))));
+            GNode g;
+            g.box = make_float4(c.lox, c.loy, c.hix, c.hiy);
+            g.mom = make_float4(ncx, ncy, tm, len);
+            g.quad = make_float4(c.sxx, c.sxy, c.syy, 0.0f);
+            g.link = make_uint4(li, ri, pl, cnt);
+            A.gnode[pidx] = g;
+        }
+        if (A.groups) {
+            // Walk groups: maximal subtrees of <= gmax bodies.  A child is one
+            // when its parent is too big; the whole tree is one when n <= gmax.
+            if (cnt > A.gmax) {
+                const uint32_t lcnt = gamma - pl + 1, rcnt = pr - gamma;
+                if (lcnt <= A.gmax) A.groups[atomicAdd(A.group_count, 1u)] = make_uint2(pl, lcnt);
+                if (rcnt <= A.gmax) A.groups[atomicAdd(A.group_count, 1u)] = make_uint2(gamma + 1, rcnt);
+            } else if (pidx == 0) {
+                A.groups[atomicAdd(A.group_count, 1u)] = make_uint2(0u, n);
+            }
+        }
+        if (!A.gnode) {
+            // Reference layout (lbvh.wgsl:12-22, split into hot and cold
+            // arrays).  With the packed records it is derived on request
+            // (ref_layout_kernel): four scattered 8-16 B writes per node
+            // fewer in every step.
+            A.node4[pidx] = make_float4(ncx, ncy, tm, len);
+            A.aabb[pidx] = make_float4(c.lox, c.loy, c.hix, c.hiy);
+            A.children[pidx] = make_uint2(li, ri);
+            A.range[pidx] = make_uint2(pl, pr);
+        }
+        A.parent[li] = pidx;
+        A.parent[ri] = pidx;
+        if (pidx == 0) {
+            A.parent[0] = kSentinel;  // lbvh.wgsl:159-161
+            return false;
+        }
+        if (IN_LOCAL) {
+            // the new node is local: its record for the sibling that may meet it here
+            const int k = (int)(pidx - B0);
+            vrec[k] = tm;
+            vrec[B + k] = ncx;
+            vrec[2 * B + k] = ncy;
+            vrec[3 * B + k] = c.lox;
+            vrec[4 * B + k] = c.loy;
+            vrec[5 * B + k] = c.hix;
+            vrec[6 * B + k] = c.hiy;
+            vrec[7 * B + k] = c.sxx;
+            vrec[8 * B + k] = c.sxy;
+            vrec[9 * B + k] = c.syy;
+        }
+        c.cm = tm; c.cx = ncx; c.cy = ncy;
+        c.l = pl;
+        c.r = pr;
+        c.dl = dpl;
+        c.dr = dpr;
+    }
+    return true;
+}
+
+// The whole climb of one thread.
+template <typename K, bool LOCAL, bool STOP>
+__device__ __forceinline__ void climb(const BuildArgs<K>& A, Climb& c, BuildShared<K>* S,
+                                      uint32_t B0) {
+    while (climb_step<K, LOCAL, STOP>(A, c, S, B0)) {
+    }
+}
+
+// Hierarchy build + fill, one thread per sorted slot.  SPLIT = false: the
+// whole climb (fused build, one kernel).  SPLIT = true: only the block-local
+// phase; threads that reach a split outside their CTA list their node in the
+// frontier and exit, and build_climb_kernel finishes the tree.  A CTA of the
+// fused build stays resident while one or two of its threads climb the
+// device-scope levels (a few L2 round trips each); the split build frees it
+// at the end of its local phase and climbs all frontier nodes side by side,
+// which pays off from a few million bodies up (measured: 2.14 -> 1.87 ms at
+// 16.8M bodies; at 800k the extra launch costs about as much as it saves).
+// (Climbing the local phase in CTA-wide rounds that pack the remaining
+// nodes into the lowest warps measured slower: the build waits on the
+// gathers of positions and masses, not on idle lanes.)
+template <typename K, bool SPLIT>
 __global__ void __launch_bounds__(kBuildBlock)
 build_fill_kernel(const BuildArgs<K> A) {
     constexpr int B = kBuildBlock;
-    __shared__ K s_key[B + 2];            // keys of slots B0-1 .. B0+B
-    __shared__ int s_d[B + 1];            // delta at boundary g = B0-1+q (between slots g, g+1)
-    __shared__ int s_wmin[2][B / 32];     // per-warp minima for the two scans
-    __shared__ int s_suf[B];              // s_suf[q] = min of s_d[q+1..B]
-    __shared__ unsigned char s_local[B + 1];
-    __shared__ uint32_t s_bound[B + 1];   // exchange slots of the local splits
-    __shared__ float s_leaf[3][B];        // leaf {m, x, y} by slot - B0
-    __shared__ float s_rec[10][B];        // local internal node {m, cx, cy, box, S} by index - B0
+    __shared__ BuildShared<K> S;
 
     const uint32_t n = A.n;
     const int t = (int)threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -134,21 +383,21 @@ build_fill_kernel(const BuildArgs<K> A) {
     // ---- boundary deltas of the CTA's slots and which splits are local ----
     for (int q = t; q < B + 2; q += B) {
         const long long g = (long long)B0 - 1 + q;
-        s_key[q] = (g >= 0 && g < (long long)n) ? __ldg(&A.keys[g]) : (K)0;
+        S.key[q] = (g >= 0 && g < (long long)n) ? __ldg(&A.keys[g]) : (K)0;
     }
-    for (int q = t; q <= B; q += B) s_bound[q] = kSentinel;
+    for (int q = t; q <= B; q += B) S.bound[q] = kSentinel;
     __syncthreads();
     for (int q = t; q <= B; q += B) {
         const long long g = (long long)B0 - 1 + q;
-        s_d[q] = (g < 0 || g >= (long long)nm1)
+        S.d[q] = (g < 0 || g >= (long long)nm1)
                      ? -1
-                     : delta_keys<K>(s_key[q], s_key[q + 1], (uint32_t)g, (uint32_t)g + 1u);
+                     : delta_keys<K>(S.key[q], S.key[q + 1], (uint32_t)g, (uint32_t)g + 1u);
     }
     __syncthreads();
     {
         const unsigned FULL = 0xFFFFFFFFu;
-        // pm = min of s_d[0..t], sm = min of s_d[t+1..B]
-        int pm = s_d[t], sm = s_d[t + 1];
+        // pm = min of d[0..t], sm = min of d[t+1..B]
+        int pm = S.d[t], sm = S.d[t + 1];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int a = __shfl_up_sync(FULL, pm, o);
@@ -156,20 +405,20 @@ build_fill_kernel(const BuildArgs<K> A) {
             if (lane >= o) pm = min(pm, a);
             if (lane + o < 32) sm = min(sm, c);
         }
-        if (lane == 31) s_wmin[0][warp] = pm;
-        if (lane == 0) s_wmin[1][warp] = sm;
+        if (lane == 31) S.wmin[0][warp] = pm;
+        if (lane == 0) S.wmin[1][warp] = sm;
         __syncthreads();
-        for (int w = 0; w < warp; ++w) pm = min(pm, s_wmin[0][w]);
-        for (int w = warp + 1; w < B / 32; ++w) sm = min(sm, s_wmin[1][w]);
-        s_suf[t] = sm;
+        for (int w = 0; w < warp; ++w) pm = min(pm, S.wmin[0][w]);
+        for (int w = warp + 1; w < B / 32; ++w) sm = min(sm, S.wmin[1][w]);
+        S.suf[t] = sm;
         __syncthreads();
         // Boundary q = t + 1 splits a local node when a smaller delta lies
-        // among s_d[0..q-1] (= pm) and among s_d[q+1..B] (= s_suf[q]).
+        // among d[0..q-1] (= pm) and among d[q+1..B] (= suf[q]).
         const int q = t + 1;
-        if (q <= B - 1) s_local[q] = (pm < s_d[q] && s_suf[q] < s_d[q]) ? 1 : 0;
+        if (q <= B - 1) S.local[q] = (pm < S.d[q] && S.suf[q] < S.d[q]) ? 1 : 0;
         if (t == 0) {
-            s_local[0] = 0;
-            s_local[B] = 0;
+            S.local[0] = 0;
+            S.local[B] = 0;
         }
         __syncthreads();
     }
@@ -179,194 +428,67 @@ build_fill_kernel(const BuildArgs<K> A) {
     const float m = __ldg(&A.mass[body]);
     const float2 p = __ldg(&A.pos[body]);
     A.node4[nm1 + i] = make_float4(p.x, p.y, m, 0.0f);  // leaf (lbvh.wgsl:179-187)
-    s_leaf[0][t] = m;
-    s_leaf[1][t] = p.x;
-    s_leaf[2][t] = p.y;
-    // Running record of the node this thread currently owns.
-    float cm = m, cx = p.x, cy = p.y;
-    float lox = p.x, loy = p.y, hix = p.x, hiy = p.y;
-    double dm = 0.0, dmx = 0.0, dmy = 0.0;  // valid when the node has >= kFp64MinBodies bodies
-    float sxx = 0.0f, sxy = 0.0f, syy = 0.0f;  // second moments about the COM (group walk)
-    uint32_t l = i, r = i;
+    S.leaf[0][t] = m;
+    S.leaf[1][t] = p.x;
+    S.leaf[2][t] = p.y;
+    Climb c;
+    c.l = i;
+    c.r = i;
     // delta at the two boundaries of the current range (-1 outside [0, n-1]);
     // a parent keeps one of them, so each level computes only one new delta.
-    int dl = s_d[t], dr = s_d[t + 1];
-    bool local = true;
-    volatile float* vrec = &s_rec[0][0];
-    volatile float* vleaf = &s_leaf[0][0];
-    while (true) {
-        const bool is_left = dr > dl;
-        const uint32_t gamma = is_left ? r : l - 1;
-        const int qg = (int)((long long)gamma - ((long long)B0 - 1));
-        local = local && qg >= 1 && qg <= B - 1 && s_local[qg];
-        uint32_t other;
-        if (local) {
-            // Shared-memory exchange: this node's record (in shared memory)
-            // is released to the CTA before the slot changes hands.
-            __threadfence_block();
-            other = atomicExch(&s_bound[qg], is_left ? l : r);
-            if (other == kSentinel) return;
-            __threadfence_block();
+    c.dl = S.d[t];
+    c.dr = S.d[t + 1];
+    c.cm = m; c.cx = p.x; c.cy = p.y;
+    c.lox = p.x; c.loy = p.y; c.hix = p.x; c.hiy = p.y;
+    c.sxx = 0.0f; c.sxy = 0.0f; c.syy = 0.0f;
+    c.dm = 0.0; c.dmx = 0.0; c.dmy = 0.0;
+    c.local = true;
+    climb<K, true, SPLIT>(A, c, &S, B0);
+}
+
+// Second kernel of the split build: one thread per frontier node (a node
+// made in the local phase, or a leaf, whose parent split is outside its
+// CTA) continues the climb with the device-scope protocol.  The node's
+// record is read back from the tree arrays the first kernel wrote; no
+// frontier node is large enough for the FP64 path (local nodes hold fewer
+// than kBuildBlock < kFp64MinBodies bodies).  Each climb ends without
+// waiting for any other thread, so a thread may take several entries.
+template <typename K>
+__global__ void __launch_bounds__(kBuildBlock)
+build_climb_kernel(const BuildArgs<K> A) {
+    const uint32_t count = *A.frontier_count;
+    const uint32_t n = A.n, nm1 = n - 1;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+        const uint2 f = A.frontier[e];
+        Climb c;
+        c.l = f.x;
+        c.r = f.y;
+        c.dl = (c.l == 0) ? -1 : delta_at(A.keys, c.l - 1, c.l);
+        c.dr = (c.r == nm1) ? -1 : delta_at(A.keys, c.r, c.r + 1);
+        c.sxx = 0.0f; c.sxy = 0.0f; c.syy = 0.0f;
+        c.dm = 0.0; c.dmx = 0.0; c.dmy = 0.0;
+        c.local = false;
+        if (c.l == c.r) {
+            const float4 leaf = A.node4[nm1 + c.l];
+            c.cm = leaf.z; c.cx = leaf.x; c.cy = leaf.y;
+            c.lox = leaf.x; c.loy = leaf.y; c.hix = leaf.x; c.hiy = leaf.y;
         } else {
-            // One acq_rel exchange releases this node's record and acquires
-            // the sibling's (release/acquire through bound[gamma]).
-            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> slot(A.bound[gamma]);
-            other = slot.exchange(is_left ? l : r, cuda::memory_order_acq_rel);
-            if (other == kSentinel) return;  // first to arrive: the sibling finishes the parent
-            slot.store(kSentinel, cuda::memory_order_relaxed);
-        }
-        const uint32_t pl = is_left ? l : other;
-        const uint32_t pr = is_left ? other : r;
-        const uint32_t li = (pl == gamma) ? nm1 + gamma : gamma;
-        const uint32_t ri = (pr == gamma + 1) ? nm1 + gamma + 1 : gamma + 1;
-        const uint32_t sib = is_left ? ri : li;
-        const uint32_t sib_cnt = is_left ? (pr - gamma) : (gamma - pl + 1);
-        const uint32_t my_cnt = r - l + 1;
-        float4 s4, sb, sq = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (local) {
-            // Sibling record from shared memory.
-            if (sib >= nm1) {
-                const int k = (int)(sib - nm1 - B0);
-                s4 = make_float4(vleaf[B + k], vleaf[2 * B + k], vleaf[k], 0.f);
-                sb = make_float4(s4.x, s4.y, s4.x, s4.y);
+            // Karras index: the range end next to the parent's split.
+            const uint32_t idx = (c.dr > c.dl) ? c.r : c.l;
+            float4 box, mom;
+            if (A.gnode) {
+                box = A.gnode[idx].box;
+                mom = A.gnode[idx].mom;
+                const float4 q = A.gnode[idx].quad;
+                c.sxx = q.x; c.sxy = q.y; c.syy = q.z;
             } else {
-                const int k = (int)(sib - B0);
-                s4 = make_float4(vrec[B + k], vrec[2 * B + k], vrec[k], 0.f);
-                sb = make_float4(vrec[3 * B + k], vrec[4 * B + k], vrec[5 * B + k], vrec[6 * B + k]);
-                sq = make_float4(vrec[7 * B + k], vrec[8 * B + k], vrec[9 * B + k], 0.f);
+                box = A.aabb[idx];
+                mom = A.node4[idx];
             }
-        } else if (sib >= nm1) {
-            // Sibling record through L2 (written by another thread in this launch).
-            s4 = __ldcg(&A.node4[sib]);
-            sb = make_float4(s4.x, s4.y, s4.x, s4.y);
-        } else if (A.gnode) {
-            sb = __ldcg(&A.gnode[sib].box);
-            s4 = __ldcg(&A.gnode[sib].mom);
-            sq = __ldcg(&A.gnode[sib].quad);
-        } else {
-            s4 = __ldcg(&A.node4[sib]);
-            sb = __ldcg(&A.aabb[sib]);
+            c.cm = mom.z; c.cx = mom.x; c.cy = mom.y;
+            c.lox = box.x; c.loy = box.y; c.hix = box.z; c.hiy = box.w;
         }
-        lox = fminf(lox, sb.x);
-        loy = fminf(loy, sb.y);
-        hix = fmaxf(hix, sb.z);
-        hiy = fmaxf(hiy, sb.w);
-        const uint32_t cnt = pr - pl + 1;
-        // Parent's boundary deltas and its own Karras index.
-        int dpl, dpr;
-        if (is_left) {
-            dpl = dl;
-            dpr = local ? s_d[(int)(pr - B0 + 1)] : ((pr == nm1) ? -1 : delta_at(A.keys, pr, pr + 1));
-        } else {
-            dpr = dr;
-            dpl = local ? s_d[(int)(pl - B0)] : ((pl == 0) ? -1 : delta_at(A.keys, pl - 1, pl));
-        }
-        const uint32_t pidx = (pl == 0 && pr == nm1) ? 0u : ((dpr > dpl) ? pr : pl);
-        float tm, ncx, ncy;
-        if (A.fp64 && cnt >= kFp64MinBodies) {
-            double sm, smx, smy;
-            if (sib_cnt >= kFp64MinBodies) {
-                const double2 s0 = __ldcg(&A.big[2 * (size_t)sib]);
-                const double2 s1 = __ldcg(&A.big[2 * (size_t)sib + 1]);
-                sm = s0.x; smx = s0.y; smy = s1.x;
-            } else {
-                sm = (double)s4.z; smx = (double)s4.z * (double)s4.x; smy = (double)s4.z * (double)s4.y;
-            }
-            if (my_cnt < kFp64MinBodies) {
-                dm = (double)cm; dmx = (double)cm * (double)cx; dmy = (double)cm * (double)cy;
-            }
-            dm += sm;
-            dmx += smx;
-            dmy += smy;
-            tm = (float)dm;
-            ncx = dm > 0.0 ? (float)(dmx / dm) : 0.0f;
-            ncy = dm > 0.0 ? (float)(dmy / dm) : 0.0f;
-            A.big[2 * (size_t)pidx] = make_double2(dm, dmx);
-            A.big[2 * (size_t)pidx + 1] = make_double2(dmy, 0.0);
-        } else {
-            float ml, mr, clx, cly, crx, cry;
-            if (is_left) { ml = cm; clx = cx; cly = cy; mr = s4.z; crx = s4.x; cry = s4.y; }
-            else { ml = s4.z; clx = s4.x; cly = s4.y; mr = cm; crx = cx; cry = cy; }
-            tm = __fadd_rn(ml, mr);
-            if (tm > 0.0f) {
-                ncx = __fdiv_rn(__fadd_rn(__fmul_rn(clx, ml), __fmul_rn(crx, mr)), tm);
-                ncy = __fdiv_rn(__fadd_rn(__fmul_rn(cly, ml), __fmul_rn(cry, mr)), tm);
-            } else {
-                ncx = 0.0f;
-                ncy = 0.0f;
-            }
-        }
-        const float len = fmaxf(__fsub_rn(hix, lox), __fsub_rn(hiy, loy));
-        if (A.gnode) {
-            // Second moments about the parent COM, left child first:
-            // S = sum_c S_c + m_c d_c d_c^T, d_c = c_c - c_parent (leaves: S_c = 0).
-            float ml, mr, lxx, lxy, lyy, rxx, rxy, ryy, dlx, dly, drx, dry;
-            if (is_left) {
-                ml = cm; lxx = sxx; lxy = sxy; lyy = syy; dlx = __fsub_rn(cx, ncx); dly = __fsub_rn(cy, ncy);
-                mr = s4.z; rxx = sq.x; rxy = sq.y; ryy = sq.z; drx = __fsub_rn(s4.x, ncx); dry = __fsub_rn(s4.y, ncy);
-            } else {
-                ml = s4.z; lxx = sq.x; lxy = sq.y; lyy = sq.z; dlx = __fsub_rn(s4.x, ncx); dly = __fsub_rn(s4.y, ncy);
-                mr = cm; rxx = sxx; rxy = sxy; ryy = syy; drx = __fsub_rn(cx, ncx); dry = __fsub_rn(cy, ncy);
-            }
-            sxx = __fadd_rn(__fadd_rn(lxx, __fmul_rn(ml, __fmul_rn(dlx, dlx))),
-                            __fadd_rn(rxx, __fmul_rn(mr, __fmul_rn(drx, drx))));
-            sxy = __fadd_rn(__fadd_rn(lxy, __fmul_rn(ml, __fmul_rn(dlx, dly))),
-                            __fadd_rn(rxy, __fmul_rn(mr, __fmul_rn(drx, dry))));
-            syy = __fadd_rn(__fadd_rn(lyy, __fmul_rn(ml, __fmul_rn(dly, dly))),
-                            __fadd_rn(ryy, __fmul_rn(mr, __fmul_rn(dry, dry))));
-            GNode g;
-            g.box = make_float4(lox, loy, hix, hiy);
-            g.mom = make_float4(ncx, ncy, tm, len);
-            g.quad = make_float4(sxx, sxy, syy, 0.0f);
-            g.link = make_uint4(li, ri, pl, cnt);
-            A.gnode[pidx] = g;
-        }
-        if (A.groups) {
-            // Walk groups: maximal subtrees of <= gmax bodies.  A child is one
-            // when its parent is too big; the whole tree is one when n <= gmax.
-            if (cnt > A.gmax) {
-                const uint32_t lcnt = gamma - pl + 1, rcnt = pr - gamma;
-                if (lcnt <= A.gmax) A.groups[atomicAdd(A.group_count, 1u)] = make_uint2(pl, lcnt);
-                if (rcnt <= A.gmax) A.groups[atomicAdd(A.group_count, 1u)] = make_uint2(gamma + 1, rcnt);
-            } else if (pidx == 0) {
-                A.groups[atomicAdd(A.group_count, 1u)] = make_uint2(0u, n);
-            }
-        }
-        if (!A.gnode) {
-            // Reference layout (lbvh.wgsl:12-22, split into hot and cold
-            // arrays).  With the packed records it is derived on request
-            // (ref_layout_kernel): four scattered 8-16 B writes per node
-            // fewer in every step.
-            A.node4[pidx] = make_float4(ncx, ncy, tm, len);
-            A.aabb[pidx] = make_float4(lox, loy, hix, hiy);
-            A.children[pidx] = make_uint2(li, ri);
-            A.range[pidx] = make_uint2(pl, pr);
-        }
-        A.parent[li] = pidx;
-        A.parent[ri] = pidx;
-        if (pidx == 0) {
-            A.parent[0] = kSentinel;  // lbvh.wgsl:159-161
-            return;
-        }
-        if (local) {
-            // the new node is local: its record for the sibling that may meet it here
-            const int k = (int)(pidx - B0);
-            vrec[k] = tm;
-            vrec[B + k] = ncx;
-            vrec[2 * B + k] = ncy;
-            vrec[3 * B + k] = lox;
-            vrec[4 * B + k] = loy;
-            vrec[5 * B + k] = hix;
-            vrec[6 * B + k] = hiy;
-            vrec[7 * B + k] = sxx;
-            vrec[8 * B + k] = sxy;
-            vrec[9 * B + k] = syy;
-        }
-        cm = tm; cx = ncx; cy = ncy;
-        l = pl;
-        r = pr;
-        dl = dpl;
-        dr = dpr;
+        climb<K, false, false>(A, c, nullptr, 0u);
     }
 }
 

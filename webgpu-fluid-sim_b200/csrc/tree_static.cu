@@ -88,7 +88,7 @@ static void launch_static(const void* codes, const uint32_t* ids, const float* m
     a.groups = nullptr;
     a.group_count = nullptr;
     a.gmax = 0u;
-    build_fill_kernel<K><<<(n + 255) / 256, 256, 0, s>>>(a);
+    build_fill_kernel<K, false><<<(n + 255) / 256, 256, 0, s>>>(a);
 }
 
 }  // namespace bh
