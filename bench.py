@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-render", action="store_true")
     return ap.parse_args()
 
 
@@ -222,6 +223,39 @@ def ensemble_cost(pkg, device: int, systems: int = 1024, steps: int = 100,
             "timing": "ensemble: CUDA events on the engine stream; loops: host clock around "
                       "synchronised calls (one handle and stream per system), same systems "
                       "and states"}
+
+
+def render_cost(pkg, device: int, width: int = 1920, height: int = 1080, frames: int = 20) -> dict:
+    """Density render of the 800k colliding-disks bodies (the reference's
+    Renderer.getCommands: clear, density splat, tone map) into a 1920 x 1080
+    headless target, timed with CUDA events on the engine's stream."""
+    import torch
+    wl = pkg.WORKLOADS["colliding-disks-800k"]
+    sim = pkg.Simulation(wl["config"], device=device)
+    sim.setNumBodies(wl["n"])
+    sim.setScenario(wl["scenario"], 1)
+    r = pkg.Renderer(sim, width, height)
+    r.setCamera(0.0, 0.0, 3.0 * width / height, 3.0)  # both disks on screen
+    for _ in range(3):
+        r.frame()
+    sim.sync()
+    ext = torch.cuda.ExternalStream(sim.getBuffers().stream, device=torch.device("cuda", device))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for _ in range(frames):
+        r.frame()
+    e1.record(ext)
+    sim.sync()
+    ms = e0.elapsed_time(e1) / frames
+    dens = r.readDensity()
+    covered = int((dens > 0).sum())
+    r.close()
+    sim.close()
+    return {"bodies": wl["n"], "canvas": [width, height], "ms_per_frame": ms,
+            "frames_per_s": 1e3 / ms, "bodies_per_s": wl["n"] / (ms / 1e3),
+            "covered_pixels": covered, "kernels_per_frame": 2,
+            "timing": "CUDA events on the engine stream, mean of %d frames" % frames}
 
 
 # ---------------------------------------------------------------- helpers
@@ -420,6 +454,9 @@ def run_own(args):
         if dist is not None:
             dist.barrier()
 
+    # FP64 diagnostics before the run (energy / momentum drift, untimed)
+    diag0 = sim.diagnostics() if rank == 0 else None
+
     # Warm-up also instantiates the profiled step graph used in the timed region.
     sim.profile_begin(max(args.warmup, 1))
     for _ in range(args.warmup):
@@ -455,6 +492,8 @@ def run_own(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     step_ms_max = float(t.item())
     value = world * n * K / (step_ms_max / 1e3)
+
+    diag1 = sim.diagnostics() if rank == 0 else None
 
     # ---- walk statistics + force error (untimed) ----
     visits, multi_inter, body_inter = sim.walk_stats()
@@ -545,6 +584,15 @@ def run_own(args):
             "cpu_baseline": cb,
             "e2e": {"value": e2e_value, "unit": "body-steps/s", "h2d_bytes_per_step": 20 * n,
                     "d2h_bytes_per_step": 16 * n, "steps": E},
+            "diagnostics": {
+                "steps": args.warmup + K,
+                "energy_drift": (diag1["total_energy"] - diag0["total_energy"])
+                                / abs(diag0["total_energy"]),
+                "momentum_change": [a - b for a, b in zip(diag1["momentum"], diag0["momentum"])],
+                "angular_momentum_drift": (diag1["angular_momentum"] - diag0["angular_momentum"])
+                                          / abs(diag0["angular_momentum"]),
+                "total_energy_start": diag0["total_energy"],
+                "how": "FP64 sums, direct-sum potential, before warm-up and after the timed steps"},
             "gpu_launches": kps * K,
             "clocks": clk,
             "wall_s_timed_region": wall,
@@ -557,6 +605,8 @@ def run_own(args):
             out["adjoint"] = adjoint_cost(pkg, local)
         if not args.no_ensemble:
             out["ensemble"] = ensemble_cost(pkg, local)
+        if not args.no_render:
+            out["render"] = render_cost(pkg, local)
         print(json.dumps(out))
     if dist is not None:
         dist.barrier()

@@ -286,6 +286,81 @@ int bh_build_hierarchy_static(const void* sorted_codes, int32_t morton_bits,
                               uint32_t* node_parent, float* node_aabb, int32_t fp64_levels,
                               void* stream);
 
+/* ---- FP64 diagnostics (extension; the reference only logs FPS, main.ts:44-49) */
+/* Conserved quantities of the current state, summed in FP64 over all bodies:
+ * total mass, centre of mass, linear momentum, angular momentum about the
+ * origin (z), kinetic energy and -- when with_potential != 0 -- the
+ * potential energy W = -G sum_{i<j} m_i m_j / sqrt(r_ij^2 + eps_ij^2) with
+ * the softening of the handle's force law (Plummer eps, or the reference's
+ * eps_ij^2 = epsMult^2 G dt max(m_i, m_j), barnes_hut.wgsl:90-92).  W is an
+ * O(N^2) direct sum (pair terms in FP32, sums in FP64; ~0.1 s at 800k bodies
+ * on a B200); potential_energy is NaN and pairs 0 when it is skipped.
+ * Synchronises the handle's stream. */
+typedef struct bh_diagnostics {
+    double total_mass;
+    double com[2];
+    double momentum[2];
+    double angular_momentum;
+    double kinetic_energy;
+    double potential_energy;
+    uint64_t pairs;
+} bh_diagnostics;
+
+int bh_diagnostics_compute(bh_sim* sim, int with_potential, bh_diagnostics* out);
+
+/* ---- density render (the reference's Renderer, src/renderer.ts:1-329) --- */
+/* A headless replacement of the two render passes of Renderer.getCommands()
+ * (renderer.ts:293-329): the density pass splats every body as the soft
+ * disc of density.wgsl:39-97 (radius 2 * radiusMultiplier pixels, weight
+ * base * exp(-10 r^2) * zoom_scale, additive), and the tone-map pass maps
+ * density to colour as tone_map.wgsl:57-84 (exposure 8, Reinhard, gamma
+ * 1/2.2, the four-stop colormap of tone_map.wgsl:24-46).  Instead of a canvas
+ * the renderer owns two device buffers in display orientation (row 0 at the
+ * top, canvas pixel (px, py) <-> world canvasPxToWorld(px + 0.5, py + 0.5)):
+ *   density[height * width]  float32, accumulated in FP32 (the reference
+ *                            blends into an r16float texture; the tone map
+ *                            here reads each density rounded to FP16 as the
+ *                            reference samples it)
+ *   image[height * width * 4] uint8 RGBA (alpha 255), unorm rounding to nearest.
+ * A pixel takes a body's contribution when its centre lies within the body's
+ * disc (|uv| <= 1, the fragment's discard test); the reference rasterises
+ * the quad around the disc first, which only differs on the disc's boundary.
+ * All work is enqueued on the simulation handle's stream; the renderer
+ * borrows the handle's position and radius buffers at each frame, so
+ * setNumBodies / setScenario need no rebind (rebindSimBuffers,
+ * renderer.ts:206-216, and setNumBodies, :219-222, have nothing to do). */
+typedef struct bh_renderer bh_renderer;
+
+/* new Renderer(...) (renderer.ts:43-61) for a width x height canvas: camera
+ * centre (0, 0), half size (10 * width / height, 10) as after the
+ * constructor's resizeCanvasToDisplaySize(). */
+int bh_renderer_create(bh_sim* sim, uint32_t width, uint32_t height, bh_renderer** out);
+int bh_renderer_destroy(bh_renderer* r);
+
+/* resizeCanvasToDisplaySize() (renderer.ts:225-252) for a new canvas size:
+ * new buffers, half size x = half size y * width / height. */
+int bh_renderer_resize(bh_renderer* r, uint32_t width, uint32_t height);
+
+/* panCamera (renderer.ts:271-277) and zoomCamera (:279-290), in canvas
+ * pixels; set/get the camera {centre x, centre y, half size x, half size y}. */
+int bh_renderer_pan(bh_renderer* r, float delta_px, float delta_py);
+int bh_renderer_zoom(bh_renderer* r, float zoom_factor, float center_px, float center_py);
+int bh_renderer_set_camera(bh_renderer* r, const float camera[4]);
+int bh_renderer_get_camera(bh_renderer* r, float camera[4]);
+
+/* getCommands(numBodies) + submit (renderer.ts:293-329, main.ts:38-41):
+ * clear, density splat of the handle's current bodies, tone map.
+ * Asynchronous on the simulation's stream. */
+int bh_renderer_frame(bh_renderer* r);
+
+/* Device buffers (valid until resize / destroy) and synchronous copies to
+ * host memory: density[height * width] floats, image[height * width * 4]. */
+int bh_renderer_get_targets(bh_renderer* r, float** density, uint8_t** image, uint32_t* width,
+                            uint32_t* height);
+int bh_renderer_read_density(bh_renderer* r, float* host);
+int bh_renderer_read_image(bh_renderer* r, uint8_t* host);
+const char* bh_renderer_last_error(bh_renderer* r);
+
 /* ---- errors ------------------------------------------------------------- */
 const char* bh_last_error(bh_sim* sim);
 const char* bh_global_last_error(void);

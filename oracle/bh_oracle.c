@@ -921,3 +921,138 @@ void orc_get_tree(const orc_state* s, uint64_t* codes, uint32_t* ids, uint32_t* 
 }
 
 uint32_t orc_num_bodies(const orc_state* s) { return s->n; }
+
+
+/* ---- density render (renderer.ts:293-329) -------------------------------- */
+
+/* density.wgsl:39-97.  Pixel-space form of the vertex + fragment stages:
+ * centre_ndc = (p - cam_centre) / cam_half (density.wgsl:60-62), radius
+ * 2 * rm pixels (:64-66), uv = (pixel centre - centre) / radius, discard
+ * |uv| > 1 (:76-78), w = exp(-k r r) with k = 10 (:81-82), zoom_scale =
+ * 1 / (1 + 0.05 max(half)) (:86-88), base 0.1 when rm > 1 else 0.02
+ * (:90-93); evaluated as (base zoom_scale) exp(-10 |uv|^2) with uv scaled
+ * by 1 / radius, as the CUDA kernel does. */
+void orc_render_density(const float cam[4], uint32_t width, uint32_t height, uint32_t n,
+                        const float* pos, const float* radius_multiplier, double* density) {
+    const float W = (float)width, H = (float)height;
+    const float zoom = cam[2] > cam[3] ? cam[2] : cam[3];
+    const float zoom_scale = 1.0f / (1.0f + 0.05f * zoom);
+    memset(density, 0, sizeof(double) * (size_t)width * height);
+    for (uint32_t b = 0; b < n; ++b) {
+        const float x = pos[2 * b], y = pos[2 * b + 1], rm = radius_multiplier[b];
+        const float cnx = (x - cam[0]) / cam[2];
+        const float cny = (y - cam[1]) / cam[3];
+        const float R = 2.0f * rm;
+        const float cpx = ((cnx + 1.0f) * 0.5f) * W;
+        const float cpy = ((cny + 1.0f) * 0.5f) * H;
+        if (!isfinite(cpx) || !isfinite(cpy) || !(R > 0.0f) || !isfinite(R)) continue;
+        float i0 = ceilf(cpx - R - 0.5f), i1 = floorf(cpx + R - 0.5f);
+        float j0 = ceilf(cpy - R - 0.5f), j1 = floorf(cpy + R - 0.5f);
+        if (i0 < 0.0f) i0 = 0.0f;
+        if (j0 < 0.0f) j0 = 0.0f;
+        if (i1 > W - 1.0f) i1 = W - 1.0f;
+        if (j1 > H - 1.0f) j1 = H - 1.0f;
+        if (!(i0 <= i1) || !(j0 <= j1)) continue;
+        const float bw = (rm > 1.0f ? 0.1f : 0.02f) * zoom_scale;
+        const float inv_r = 1.0f / R;
+        for (uint32_t j = (uint32_t)j0; j <= (uint32_t)j1; ++j) {
+            for (uint32_t i = (uint32_t)i0; i <= (uint32_t)i1; ++i) {
+                const float ux = (((float)i + 0.5f) - cpx) * inv_r;
+                const float uy = (((float)j + 0.5f) - cpy) * inv_r;
+                const float r2 = ux * ux + uy * uy;
+                if (r2 > 1.0f) continue;
+                density[(size_t)j * width + i] += (double)(bw * expf(-10.0f * r2));
+            }
+        }
+    }
+}
+
+static float orc_mix(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+
+/* tone_map.wgsl:24-46 */
+void orc_colormap(float t, float rgb[3]) {
+    static const float c[4][3] = {{0.0f, 0.0f, 0.0f}, {0.10f, 0.20f, 0.90f},
+                                  {0.20f, 0.90f, 0.90f}, {1.0f, 1.0f, 1.0f}};
+    const float x = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
+    int seg;
+    float a;
+    if (x < 0.33f) {
+        seg = 0;
+        a = x / 0.33f;
+    } else if (x < 0.66f) {
+        seg = 1;
+        a = (x - 0.33f) / 0.33f;
+    } else {
+        seg = 2;
+        a = (x - 0.66f) / 0.34f;
+    }
+    for (int k = 0; k < 3; ++k) rgb[k] = orc_mix(c[seg][k], c[seg + 1][k], a);
+}
+
+static uint8_t orc_unorm8(float c) {
+    const float v = (c < 0.0f ? 0.0f : (c > 1.0f ? 1.0f : c)) * 255.0f;
+    return (uint8_t)lrintf(v);
+}
+
+/* tone_map.wgsl:63-84 (the r16float texel is the density rounded to FP16) */
+void orc_tone_map(uint32_t pixels, const float* density, uint8_t* rgba) {
+    const float gamma = (float)(1.0 / 2.2);
+    for (uint32_t p = 0; p < pixels; ++p) {
+        const float d = (float)(_Float16)density[p];
+        const float x = 8.0f * d;
+        const float mapped = x / (1.0f + x);
+        const float m = mapped < 0.0f ? 0.0f : (mapped > 1.0f ? 1.0f : mapped);
+        float rgb[3];
+        orc_colormap(powf(m, gamma), rgb);
+        rgba[4 * (size_t)p] = orc_unorm8(rgb[0]);
+        rgba[4 * (size_t)p + 1] = orc_unorm8(rgb[1]);
+        rgba[4 * (size_t)p + 2] = orc_unorm8(rgb[2]);
+        rgba[4 * (size_t)p + 3] = 255;
+    }
+}
+
+
+/* ---- FP64 diagnostics ----------------------------------------------------- */
+
+void orc_diagnostics_fp64(const orc_params* p, uint32_t n, const float* mass, const float* pos,
+                          const float* vel, double out[8]) {
+    double a[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t i = 0; i < n; ++i) {
+        const double m = mass[i], x = pos[2 * i], y = pos[2 * i + 1];
+        const double vx = vel[2 * i], vy = vel[2 * i + 1];
+        a[0] += m;
+        a[1] += m * x;
+        a[2] += m * y;
+        a[3] += m * vx;
+        a[4] += m * vy;
+        a[5] += m * (x * vy - y * vx);
+        a[6] += 0.5 * m * (vx * vx + vy * vy);
+    }
+    const double G = p->grav_constant;
+    /* the engine forms this coefficient in f32 (epsMult^2 G dt) */
+    const double coef = (double)(p->epsilon_multiplier * p->epsilon_multiplier * p->grav_constant *
+                                 p->delta_time);
+    const double e2p = (double)p->plummer_eps * p->plummer_eps;
+    double W = 0.0;
+#pragma omp parallel for reduction(+ : W) schedule(dynamic, 64)
+    for (uint32_t i = 0; i < n; ++i) {
+        const double mi = mass[i], xi = pos[2 * i], yi = pos[2 * i + 1];
+        double s = 0.0;
+        for (uint32_t j = i + 1; j < n; ++j) {
+            const double mj = mass[j];
+            const double dx = pos[2 * j] - xi, dy = pos[2 * j + 1] - yi;
+            const double e2 = p->softening == 1 ? e2p : coef * (mi > mj ? mi : mj);
+            const double r2 = dx * dx + dy * dy + e2;
+            if (r2 > 0.0) s += mj / sqrt(r2);
+        }
+        W += mi * s;
+    }
+    out[0] = a[0];
+    out[1] = a[0] > 0.0 ? a[1] / a[0] : 0.0;
+    out[2] = a[0] > 0.0 ? a[2] / a[0] : 0.0;
+    out[3] = a[3];
+    out[4] = a[4];
+    out[5] = a[5];
+    out[6] = a[6];
+    out[7] = -G * W;
+}

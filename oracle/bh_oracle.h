@@ -146,6 +146,27 @@ void orc_get_tree(const orc_state* s, uint64_t* codes, uint32_t* ids, uint32_t* 
                   float* length);
 uint32_t orc_num_bodies(const orc_state* s);
 
+/* Density render (next to the path: the reference's Renderer, renderer.ts).
+ * cam = {centre x, centre y, half size x, half size y}; buffers in display
+ * orientation (row 0 at the top, world y growing downwards as in
+ * renderer.ts:262-269 canvasPxToWorld).
+ * orc_render_density: density.wgsl:39-97 -- every body adds
+ *   base * exp(-10 r^2) * zoom_scale to each pixel centre within r = |uv| <= 1
+ *   of its disc of 2 * radius_multiplier pixels; summed in FP64 in body order.
+ * orc_tone_map: tone_map.wgsl:57-84 -- density rounded to FP16, exposure 8,
+ *   Reinhard, gamma 1/2.2, colormap (tone_map.wgsl:24-46), RGBA8. */
+void orc_render_density(const float cam[4], uint32_t width, uint32_t height, uint32_t n,
+                        const float* pos, const float* radius_multiplier, double* density);
+void orc_tone_map(uint32_t pixels, const float* density, uint8_t* rgba);
+/* colormap(t) of tone_map.wgsl:24-46 (rgb). */
+void orc_colormap(float t, float rgb[3]);
+
+/* FP64 diagnostics: out = {M, COM x, COM y, P x, P y, Lz, K, W}; W is the
+ * direct pair sum -G sum_{i<j} m_i m_j / sqrt(r^2 + eps_ij^2) with the
+ * softening of p (Plummer, or barnes_hut.wgsl:90-92's mass-dependent eps). */
+void orc_diagnostics_fp64(const orc_params* p, uint32_t n, const float* mass, const float* pos,
+                          const float* vel, double out[8]);
+
 /* OpenMP thread count the parallel paths use. */
 int orc_max_threads(void);
 

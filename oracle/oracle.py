@@ -84,6 +84,11 @@ def load() -> ctypes.CDLL:
                                                     ctypes.c_uint32, _P, _P, _P]),
         "orc_force_vjp_fp64": (None, [P, ctypes.c_uint32, _P, _P, _P, _P, _P]),
         "orc_max_threads": (ctypes.c_int, []),
+        "orc_render_density": (None, [_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _P, _P,
+                                      _P]),
+        "orc_tone_map": (None, [ctypes.c_uint32, _P, _P]),
+        "orc_colormap": (None, [ctypes.c_float, _P]),
+        "orc_diagnostics_fp64": (None, [P, ctypes.c_uint32, _P, _P, _P, _P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -226,6 +231,45 @@ def force_vjp_fp64(p: OrcParams, mass, pos, abar):
     mb = np.zeros(n, np.float64)
     lib.orc_force_vjp_fp64(ctypes.byref(p), n, _p(mass), _p(pos), _p(abar), _p(xb), _p(mb))
     return xb, mb
+
+
+def diagnostics_fp64(p: OrcParams, mass, pos, vel) -> dict:
+    """FP64 conserved quantities: M, COM, P, Lz, K, W (direct pair sum)."""
+    lib = load()
+    mass = f32(mass)
+    out = np.zeros(8, np.float64)
+    lib.orc_diagnostics_fp64(ctypes.byref(p), mass.size, _p(mass), _p(f32(pos, (-1, 2))),
+                             _p(f32(vel, (-1, 2))), _p(out))
+    return dict(total_mass=out[0], com=out[1:3], momentum=out[3:5], angular_momentum=out[5],
+                kinetic_energy=out[6], potential_energy=out[7])
+
+
+def render_density(cam, width: int, height: int, pos, radius_multiplier) -> np.ndarray:
+    """density.wgsl restated: (height, width) FP64 density, display orientation."""
+    lib = load()
+    cam = np.ascontiguousarray(cam, np.float32)
+    pos = f32(pos, (-1, 2))
+    rm = f32(radius_multiplier)
+    out = np.zeros((height, width), np.float64)
+    lib.orc_render_density(_p(cam), width, height, rm.size, _p(pos), _p(rm), _p(out))
+    return out
+
+
+def tone_map(density) -> np.ndarray:
+    """tone_map.wgsl restated: RGBA8 image of a (height, width) float32 density."""
+    lib = load()
+    d = f32(density)
+    h, w = np.shape(density)
+    out = np.zeros((h, w, 4), np.uint8)
+    lib.orc_tone_map(h * w, _p(d), _p(out))
+    return out
+
+
+def colormap(t: float) -> np.ndarray:
+    lib = load()
+    out = np.zeros(3, np.float32)
+    lib.orc_colormap(float(t), _p(out))
+    return out
 
 
 REF_LIB = os.path.join(HERE, "_ref", "libref_wgsl.so")

@@ -7,5 +7,7 @@ repository root on ``sys.path``.
 """
 from ._lib import BhError, load  # noqa: F401
 from .config import WORKLOADS, Config, getDefaultConfig  # noqa: F401
+from .render import RenderCommand, Renderer  # noqa: F401
+from .runlog import RunLog  # noqa: F401
 from .simulation import (SCENARIOS, CommandBuffer, Ensemble, SimBuffers,  # noqa: F401
                          Simulation, ensemble_sizes, generate_scenario, submit)

@@ -86,6 +86,18 @@ class bh_buffers(ctypes.Structure):
     ]
 
 
+class bh_diagnostics(ctypes.Structure):
+    _fields_ = [
+        ("total_mass", ctypes.c_double),
+        ("com", ctypes.c_double * 2),
+        ("momentum", ctypes.c_double * 2),
+        ("angular_momentum", ctypes.c_double),
+        ("kinetic_energy", ctypes.c_double),
+        ("potential_energy", ctypes.c_double),
+        ("pairs", ctypes.c_uint64),
+    ]
+
+
 # name -> (restype, argtypes); every symbol declared in include/bh.h
 _P = ctypes.c_void_p
 _F = ctypes.POINTER(ctypes.c_float)
@@ -127,6 +139,21 @@ SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_float), _P, _P, _P]),
     "bh_build_hierarchy_static": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _P, ctypes.c_uint32,
                                                  _P, _P, _P, _P, ctypes.c_int32, _P]),
+    "bh_diagnostics_compute": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(bh_diagnostics)]),
+    "bh_renderer_create": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_P)]),
+    "bh_renderer_destroy": (ctypes.c_int, [_P]),
+    "bh_renderer_resize": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32]),
+    "bh_renderer_pan": (ctypes.c_int, [_P, ctypes.c_float, ctypes.c_float]),
+    "bh_renderer_zoom": (ctypes.c_int, [_P, ctypes.c_float, ctypes.c_float, ctypes.c_float]),
+    "bh_renderer_set_camera": (ctypes.c_int, [_P, _F]),
+    "bh_renderer_get_camera": (ctypes.c_int, [_P, _F]),
+    "bh_renderer_frame": (ctypes.c_int, [_P]),
+    "bh_renderer_get_targets": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P),
+                                               ctypes.POINTER(ctypes.c_uint32),
+                                               ctypes.POINTER(ctypes.c_uint32)]),
+    "bh_renderer_read_density": (ctypes.c_int, [_P, _P]),
+    "bh_renderer_read_image": (ctypes.c_int, [_P, _P]),
+    "bh_renderer_last_error": (ctypes.c_char_p, [_P]),
     "bh_last_error": (ctypes.c_char_p, [_P]),
     "bh_global_last_error": (ctypes.c_char_p, []),
     "bh_version": (ctypes.c_char_p, []),

@@ -154,7 +154,7 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
                 for (int k = 0; k < BPL; ++k) {
                     if (!ok[k]) continue;
                     const float rx = mom.x - bx[k], ry = mom.y - by[k];
-                    const float s = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, eps2)));
+                    const float s = rsqrt_ftz(fmaf(rx, rx, fmaf(ry, ry, eps2)));
                     const float s2 = s * s, s3 = s * s2, s5 = s3 * s2;
                     const float ar = abx[k] * rx + aby[k] * ry;
                     float rbx = mom.z * (s3 * abx[k] - 3.0f * s5 * ar * rx);
@@ -210,7 +210,7 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
                 for (int k = 0; k < BPL; ++k) {
                     if (!ok[k] || sj == base + (uint32_t)k * 32u + (uint32_t)lane) continue;
                     const float rx = o.x - bx[k], ry = o.y - by[k];
-                    const float s = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, eps2)));
+                    const float s = rsqrt_ftz(fmaf(rx, rx, fmaf(ry, ry, eps2)));
                     const float s3 = s * s * s, s5 = s3 * s * s;
                     const float ar = abx[k] * rx + aby[k] * ry;
                     const float rbx = o.z * (s3 * abx[k] - 3.0f * s5 * ar * rx);

@@ -62,6 +62,15 @@ __device__ __forceinline__ bool group_accepts(const float4& box, float cx, float
     return __fmul_rn(L, L) < __fmul_rn(th2, d2) && (sx > 0.0f || sy > 0.0f);
 }
 
+// Reciprocal square root with subnormal inputs flushed to zero, which drops
+// the subnormal-input handling around each hardware rsqrt.  It changes a
+// result only for |r|^2 + eps^2 below 1.2e-38 (coincident bodies without
+// softening), where the force is not finite either way.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 // Group-walk stack and list capacities (per warp).
 constexpr int kGroupStack = 1024;
 constexpr int kGroupDfsAt = kGroupStack - 128;  // switch to one node per step above this depth
@@ -146,6 +155,17 @@ struct DeviceBuffers {
     const uint32_t* sys_off = nullptr;  // E+1 body offsets (original order = sorted order by system)
     const uint32_t* body_sys = nullptr; // n: system of each body (original order)
     uint32_t* sys_bbox = nullptr;       // 4E ordered-int max of {-minx, -miny, maxx, maxy}
+};
+
+// Body buffers of a simulation handle (renderer, diagnostics).
+struct BodyView {
+    const float* mass = nullptr;
+    const float2* pos = nullptr;
+    const float2* vel = nullptr;
+    const float* radius = nullptr;
+    uint32_t n = 0;
+    cudaStream_t stream = nullptr;
+    int device = 0;
 };
 
 // ---- launchers (all asynchronous on `s`) --------------------------------

@@ -74,6 +74,22 @@ namespace bh {
 void set_global_error(const std::string& msg) { g_err = msg; }
 }  // namespace bh
 
+namespace bh {
+// The handle's body buffers without side effects (bh_get_buffers also
+// refreshes the reference node layout); false for a null handle.
+bool sim_body_view(const bh_sim* s, BodyView* out) {
+    if (!s || !out) return false;
+    out->mass = s->b.mass;
+    out->pos = s->b.pos;
+    out->vel = s->b.vel;
+    out->radius = s->b.radius;
+    out->n = s->b.n;
+    out->stream = s->stream;
+    out->device = s->device;
+    return true;
+}
+}  // namespace bh
+
 static int fail(bh_sim* s, int code, const std::string& msg) {
     if (s) s->err = msg;
     g_err = msg;
@@ -313,8 +329,14 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
         while (sb < 32 && ((E - 1) >> sb)) ++sb;
         int passes = (32 + sb + 7) / 8;
         b.sort_passes = passes + (passes & 1);
-        BH_CUDA(s, cudaMemcpy((void*)b.sys_off, off.data(), 4 * (size_t)(E + 1), cudaMemcpyHostToDevice));
-        BH_CUDA(s, cudaMemcpy((void*)b.body_sys, bsys.data(), 4 * (size_t)nb, cudaMemcpyHostToDevice));
+        // On the handle's stream, after the arena memset above: the stream is
+        // non-blocking, so a copy on the legacy stream would not be ordered
+        // against that memset (which could then clear the offsets).
+        BH_CUDA(s, cudaMemcpyAsync((void*)b.sys_off, off.data(), 4 * (size_t)(E + 1),
+                                   cudaMemcpyHostToDevice, s->stream));
+        BH_CUDA(s, cudaMemcpyAsync((void*)b.body_sys, bsys.data(), 4 * (size_t)nb,
+                                   cudaMemcpyHostToDevice, s->stream));
+        BH_CUDA(s, cudaStreamSynchronize(s->stream));
     }
     BH_CUDA(s, cudaStreamSynchronize(s->stream));
     s->acc_valid = false;
@@ -454,15 +476,16 @@ static cudaEvent_t* prof_slot(bh_sim* s) {
 
 static int check_device_errors(bh_sim* s) {
     uint32_t e = 0;
-    BH_CUDA(s, cudaMemcpy(&e, s->b.err, sizeof(e), cudaMemcpyDeviceToHost));
+    BH_CUDA(s, cudaMemcpyAsync(&e, s->b.err, sizeof(e), cudaMemcpyDeviceToHost, s->stream));
+    BH_CUDA(s, cudaStreamSynchronize(s->stream));
     if (e == 0) return BH_OK;
-    BH_CUDA(s, cudaMemset(s->b.err, 0, sizeof(uint32_t)));
+    BH_CUDA(s, cudaMemsetAsync(s->b.err, 0, sizeof(uint32_t), s->stream));
     std::string msg = "device check failed:";
     if (e & bh::kErrLookbackSpin) msg += " sort look-back gave up waiting;";
     if (e & bh::kErrStackOverflow) msg += " walk stack full (children dropped);";
     if (e & bh::kErrTreeSpin) msg += " tree build gave up waiting;";
     // Restore the build's exchange slots so the next step starts clean.
-    if (s->b.n > 1) BH_CUDA(s, cudaMemset(s->b.bound, 0xFF, sizeof(uint32_t) * (s->b.n - 1)));
+    if (s->b.n > 1) BH_CUDA(s, cudaMemsetAsync(s->b.bound, 0xFF, sizeof(uint32_t) * (s->b.n - 1), s->stream));
     return fail(s, BH_ERR_DEVICE_CHECK, msg);
 }
 
@@ -1064,8 +1087,8 @@ extern "C" int bh_read_buffer(bh_sim* s, const char* name, void* host, size_t by
     if (bytes > cap) return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_read_buffer: size above the buffer");
     if (b.gnode && (nm == "node4" || nm == "node_children" || nm == "node_aabb"))
         bh::launch_ref_layout(b, s->stream);
+    if (bytes) BH_CUDA(s, cudaMemcpyAsync(host, src, bytes, cudaMemcpyDeviceToHost, s->stream));
     BH_CUDA(s, cudaStreamSynchronize(s->stream));
-    if (bytes) BH_CUDA(s, cudaMemcpy(host, src, bytes, cudaMemcpyDeviceToHost));
     return BH_OK;
 }
 

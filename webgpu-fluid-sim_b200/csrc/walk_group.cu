@@ -85,15 +85,6 @@ __device__ __forceinline__ f2x fma2(f2x a, f2x b, f2x c) {
     asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
     return r;
 }
-// Reciprocal square root with subnormal inputs flushed to zero, which drops
-// the subnormal-input handling around each hardware rsqrt.  It changes a
-// result only for |r|^2 + eps^2 below 1.2e-38 (coincident bodies without
-// softening), where the force is not finite either way.
-__device__ __forceinline__ float rsqrt_ftz(float x) {
-    float r;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
 __device__ __forceinline__ f2x rsqrt2(f2x v) {
     float lo, hi;
     upk(v, lo, hi);

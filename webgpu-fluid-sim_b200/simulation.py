@@ -243,6 +243,22 @@ class Simulation:
                                             ctypes.byref(b)))
         return int(v.value), int(m.value), int(b.value)
 
+    def diagnostics(self, potential: bool = True) -> dict:
+        """FP64 conserved quantities of the current state (bh_diagnostics_compute):
+        total mass, centre of mass, momentum, angular momentum (z), kinetic and
+        -- with ``potential`` -- direct-sum potential energy."""
+        d = _lib.bh_diagnostics()
+        self._check(self._lib.bh_diagnostics_compute(self._h, 1 if potential else 0,
+                                                     ctypes.byref(d)))
+        out = dict(total_mass=d.total_mass, com=[d.com[0], d.com[1]],
+                   momentum=[d.momentum[0], d.momentum[1]],
+                   angular_momentum=d.angular_momentum, kinetic_energy=d.kinetic_energy)
+        if potential:
+            out["potential_energy"] = d.potential_energy
+            out["total_energy"] = d.kinetic_energy + d.potential_energy
+            out["pairs"] = int(d.pairs)
+        return out
+
     def kernels_per_step(self) -> int:
         k = ctypes.c_uint32()
         self._check(self._lib.bh_kernels_per_step(self._h, ctypes.byref(k)))
