@@ -225,6 +225,46 @@ def ensemble_cost(pkg, device: int, systems: int = 1024, steps: int = 100,
                       "and states"}
 
 
+def generate_cost(pkg, device: int, name: str = "gaussian-mixture", n: int = 16_777_216) -> dict:
+    """Initial conditions for the 16.8M-body Gaussian mixture: the host
+    generator (one PCG32 stream, then the 400 MB upload a step needs) against
+    the GPU generator (one stream per body) into device arrays."""
+    import ctypes
+    import torch
+    dev = torch.device("cuda", device)
+    t0 = time.perf_counter()
+    mass, pos, vel, rad = pkg.generate_scenario(name, n, 1)
+    host_s = time.perf_counter() - t0
+    lib = pkg.load()
+    bufs = [torch.empty(k * n, dtype=torch.float32, device=dev) for k in (1, 2, 2, 1)]
+    stream = torch.cuda.current_stream(dev)
+    args = [ctypes.c_void_p(b.data_ptr()) for b in bufs]
+    lib.bh_generate_scenario_device(name.encode(), n, 1, 1.0, *args,
+                                    ctypes.c_void_p(stream.cuda_stream))  # warm-up
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    rc = lib.bh_generate_scenario_device(name.encode(), n, 1, 1.0, *args,
+                                         ctypes.c_void_p(stream.cuda_stream))
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    h = [torch.from_numpy(a.reshape(-1)).pin_memory() for a in (mass, pos, vel, rad)]
+    pin_s = time.perf_counter() - t0
+    u0 = torch.cuda.Event(enable_timing=True)
+    u1 = torch.cuda.Event(enable_timing=True)
+    u0.record(stream)
+    for b, a in zip(bufs, h):
+        b.copy_(a, non_blocking=True)
+    u1.record(stream)
+    torch.cuda.synchronize(dev)
+    return {"scenario": name, "bodies": n, "host_generate_s": host_s,
+            "host_upload_ms": u0.elapsed_time(u1), "host_pin_s": pin_s,
+            "device_generate_ms": e0.elapsed_time(e1) if rc == 0 else None,
+            "timing": "host: wall clock, one thread; upload from page-locked memory and the GPU "
+                      "generator: CUDA events"}
+
+
 def render_cost(pkg, device: int, width: int = 1920, height: int = 1080, frames: int = 20) -> dict:
     """Density render of the 800k colliding-disks bodies (the reference's
     Renderer.getCommands: clear, density splat, tone map) into a 1920 x 1080
@@ -607,6 +647,8 @@ def run_own(args):
             out["ensemble"] = ensemble_cost(pkg, local)
         if not args.no_render:
             out["render"] = render_cost(pkg, local)
+        if not args.no_secondary:
+            out["generate"] = generate_cost(pkg, local)
         print(json.dumps(out))
     if dist is not None:
         dist.barrier()

@@ -167,6 +167,25 @@ int bh_get_num_bodies(bh_sim* sim, uint32_t* out); /* getNumBodies() (simulation
  * "node_aabb". */
 int bh_read_buffer(bh_sim* sim, const char* name, void* host, size_t bytes);
 
+/* ---- scenarios generated on the GPU (extension) -------------------------- */
+/* Same names, distributions and formulas as bh_set_scenario, generated on
+ * the GPU: body i draws from its own PCG32 stream (sequence selector
+ * splitmix64(i), state seeded by `seed`), in FP64, stored as FP32, so no host
+ * arrays and no upload are involved (16.8M bodies in a few milliseconds).
+ * The sample differs from bh_set_scenario's for the same seed (that one
+ * draws all bodies from one sequential stream).  Reallocates the buffers
+ * like bh_set_scenario; later bh_set_num_bodies calls regenerate on the GPU
+ * until bh_set_scenario is called again.  Gaussian-mixture masses are
+ * normalised by an FP64 total whose last bits follow the GPU's SM count. */
+int bh_set_scenario_device(bh_sim* sim, const char* name, uint64_t seed);
+
+/* The same generators on caller-owned device arrays (mass[n], pos[2n],
+ * vel[2n], radius_multiplier[n] or NULL), enqueued on `stream` (a
+ * cudaStream_t) of the current device. */
+int bh_generate_scenario_device(const char* name, uint32_t n, uint64_t seed, float grav_constant,
+                                float* mass, float* pos, float* vel, float* radius_multiplier,
+                                void* stream);
+
 /* ---- host-side scenario generation (no device work) --------------------- */
 /* Fills mass[n], pos[2n], vel[2n] and (optionally) radius_multiplier[n] with
  * the named scenario, exactly as bh_set_scenario does before its upload. */

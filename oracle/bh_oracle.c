@@ -1056,3 +1056,198 @@ void orc_diagnostics_fp64(const orc_params* p, uint32_t n, const float* mass, co
     out[6] = a[6];
     out[7] = -G * W;
 }
+
+
+/* ---- scenarios with one PCG32 stream per body ------------------------------ */
+
+#define ORC_PI 3.14159265358979323846 /* M_PI of <math.h> (not declared under -std=c11) */
+
+typedef struct orc_pcg {
+    uint64_t state, inc;
+} orc_pcg;
+
+static uint32_t orc_pcg_next(orc_pcg* r) {
+    const uint64_t old = r->state;
+    r->state = old * 6364136223846793005ULL + r->inc;
+    const uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    const uint32_t rot = (uint32_t)(old >> 59u);
+    return (xs >> rot) | (xs << ((32u - rot) & 31u));
+}
+
+/* PCG32 (O'Neill 2014): increment 2 seq + 1, state advanced, seeded, advanced */
+static orc_pcg orc_pcg_make(uint64_t seed, uint64_t seq) {
+    orc_pcg r = {0, (seq << 1u) | 1u};
+    orc_pcg_next(&r);
+    r.state += seed;
+    orc_pcg_next(&r);
+    return r;
+}
+
+static double orc_pcg_uniform(orc_pcg* r) {
+    const uint64_t a = orc_pcg_next(r) >> 5, b = orc_pcg_next(r) >> 6;
+    return (double)(a * 67108864ULL + b) * (1.0 / 9007199254740992.0);
+}
+
+static double orc_pcg_normal(orc_pcg* r) {
+    double u1 = orc_pcg_uniform(r);
+    const double u2 = orc_pcg_uniform(r);
+    if (u1 < 1e-300) u1 = 1e-300;
+    return sqrt(-2.0 * log(u1)) * cos(2.0 * ORC_PI * u2);
+}
+
+static uint64_t orc_splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ULL;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+    return x ^ (x >> 31);
+}
+
+static void orc_put(float* mass, float* pos, float* vel, uint32_t i, double m, double x, double y,
+                    double vx, double vy) {
+    mass[i] = (float)m;
+    pos[2 * i] = (float)x;
+    pos[2 * i + 1] = (float)y;
+    vel[2 * i] = (float)vx;
+    vel[2 * i + 1] = (float)vy;
+}
+
+#define ORC_MIX_K 64
+
+static void orc_mixture_point(uint64_t seed, const double* cx, const double* cy, const double* sig,
+                              uint32_t j, float* x, float* y) {
+    for (;;) {
+        orc_pcg r = orc_pcg_make(seed, orc_splitmix64(j));
+        (void)orc_pcg_normal(&r); /* the body's mass draw */
+        if (j > 0 && orc_pcg_uniform(&r) < 0.01) {
+            j = (uint32_t)(orc_pcg_uniform(&r) * (double)j);
+            continue;
+        }
+        int k = (int)(orc_pcg_uniform(&r) * ORC_MIX_K);
+        if (k >= ORC_MIX_K) k = ORC_MIX_K - 1;
+        const double px = cx[k] + sig[k] * orc_pcg_normal(&r);
+        const double py = cy[k] + sig[k] * orc_pcg_normal(&r);
+        *x = (float)px;
+        *y = (float)py;
+        return;
+    }
+}
+
+int orc_generate_per_body(const char* name, uint32_t n, uint64_t seed, double G, float* mass,
+                          float* pos, float* vel, float* radius) {
+    int sc;
+    if (!name) return -1;
+    if (!strcmp(name, "default")) sc = 0;
+    else if (!strcmp(name, "two-clusters")) sc = 1;
+    else if (!strcmp(name, "planetary-disk")) sc = 2;
+    else if (!strcmp(name, "uniform-disk-kepler")) sc = 3;
+    else if (!strcmp(name, "colliding-disks")) sc = 4;
+    else if (!strcmp(name, "gaussian-mixture")) sc = 5;
+    else if (!strcmp(name, "plummer-projection")) sc = 6;
+    else return -1;
+    double cx[ORC_MIX_K], cy[ORC_MIX_K], sig[ORC_MIX_K];
+    if (sc == 5) {
+        orc_pcg r = orc_pcg_make(seed, 0x5851f42d4c957f2dULL);
+        for (int k = 0; k < ORC_MIX_K; ++k) {
+            cx[k] = -4.0 + 8.0 * orc_pcg_uniform(&r);
+            cy[k] = -4.0 + 8.0 * orc_pcg_uniform(&r);
+            sig[k] = exp(log(1e-3) + (log(0.5) - log(1e-3)) * orc_pcg_uniform(&r));
+        }
+    }
+    double total = 0.0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (radius) radius[i] = 1.0f;
+        orc_pcg r = orc_pcg_make(seed, orc_splitmix64(i));
+        if (sc == 0) { /* simulation.ts:243-266 */
+            const double angle = orc_pcg_uniform(&r) * 2.0 * ORC_PI;
+            const double rr = 5.0 * sqrt(orc_pcg_uniform(&r));
+            const double x = rr * cos(angle), y = rr * sin(angle);
+            const double dist = sqrt(x * x + y * y);
+            const double speed = 0.1 * sqrt(G * (double)n / dist);
+            orc_put(mass, pos, vel, i, 1.0, x, y, -speed * (y / dist), speed * (x / dist));
+        } else if (sc == 1) { /* simulation.ts:267-306 */
+            const double angle = orc_pcg_uniform(&r) * 2.0 * ORC_PI;
+            const double rr = 3.0 * sqrt(orc_pcg_uniform(&r));
+            const double xb = rr * cos(angle), yb = rr * sin(angle);
+            const int first = (double)i < (double)n / 2.0;
+            const double dist = sqrt(xb * xb + yb * yb);
+            const double speed = 0.12 * sqrt(G * ((double)n / 2.0) / dist);
+            orc_put(mass, pos, vel, i, 1.0, first ? xb - 15.0 : xb + 15.0, yb,
+                    first ? -speed * (yb / dist) : speed * (yb / dist),
+                    first ? speed * (xb / dist) : -speed * (xb / dist));
+        } else if (sc == 2) { /* simulation.ts:308-361 */
+            const double central = 1000.0, planet = 10.0;
+            if (i == 0) {
+                orc_put(mass, pos, vel, i, central, 0.0, 0.0, 0.0, 0.0);
+                if (radius) radius[i] = 12.0f;
+            } else if (i == 1) {
+                orc_put(mass, pos, vel, i, planet, 2.5, 0.0, 0.0, 0.8 * sqrt(G * central / 2.5));
+                if (radius) radius[i] = 5.0f;
+            } else if (i == 2) {
+                orc_put(mass, pos, vel, i, planet, 12.0, 0.0, 0.0, sqrt(G * central / 12.5));
+                if (radius) radius[i] = 5.0f;
+            } else {
+                const double angle = orc_pcg_uniform(&r) * 2.0 * ORC_PI;
+                const double rr = sqrt(orc_pcg_uniform(&r) * (15.0 * 15.0 - 0.1 * 0.1) + 0.1 * 0.1);
+                const double x = rr * cos(angle), y = rr * sin(angle);
+                const double dist = sqrt(x * x + y * y);
+                const double speed = 1.01 * sqrt(G * central / (2.0 + dist));
+                orc_put(mass, pos, vel, i, central / (100.0 * (double)n), x, y, -speed * (y / dist),
+                        speed * (x / dist));
+            }
+        } else if (sc == 3) { /* uniform disk, Keplerian about M(<r) = r^2 */
+            const double angle = orc_pcg_uniform(&r) * 2.0 * ORC_PI;
+            const double rr = sqrt(orc_pcg_uniform(&r));
+            const double x = rr * cos(angle), y = rr * sin(angle);
+            const double v = sqrt(G * rr * rr / (rr > 1e-12 ? rr : 1e-12));
+            const double c = rr > 0 ? x / rr : 1.0, s = rr > 0 ? y / rr : 0.0;
+            orc_put(mass, pos, vel, i, 1.0 / (double)n, x, y, -v * s, v * c);
+        } else if (sc == 4) { /* two colliding exponential disks */
+            const double h = 0.2, rmax = 10.0 * h, md = 1.0 / 2.2, mc = 0.1 * md;
+            const uint32_t half = n / 2;
+            const int gal = i < half ? 0 : 1;
+            const uint32_t lo = gal == 0 ? 0 : half, hi = gal == 0 ? half : n, cnt = hi - lo;
+            const double gx = gal == 0 ? 1.5 : -1.5;
+            const double bvx = gal == 0 ? -0.3 : 0.3, bvy = gal == 0 ? 0.1 : -0.1;
+            if (i == lo) {
+                orc_put(mass, pos, vel, i, cnt > 1 ? mc : md + mc, gx, 0.0, bvx, bvy);
+                continue;
+            }
+            double R = rmax;
+            for (int t = 0; t < 64; ++t) {
+                double u1 = orc_pcg_uniform(&r), u2 = orc_pcg_uniform(&r);
+                if (u1 < 1e-300) u1 = 1e-300;
+                if (u2 < 1e-300) u2 = 1e-300;
+                R = -h * log(u1 * u2);
+                if (R <= rmax) break;
+            }
+            if (R > rmax) R = rmax;
+            const double angle = orc_pcg_uniform(&r) * 2.0 * ORC_PI;
+            const double x = R * cos(angle), y = R * sin(angle);
+            const double menc = mc + md * (1.0 - (1.0 + R / h) * exp(-R / h));
+            const double Rs = R > 1e-6 ? R : 1e-6;
+            const double v = sqrt(G * menc / Rs);
+            orc_put(mass, pos, vel, i, md / (double)(cnt - 1), gx + x, y, bvx - v * (y / Rs),
+                    bvy + v * (x / Rs));
+        } else if (sc == 5) { /* Gaussian mixture, 1% duplicates, log-normal masses */
+            const double m = exp(orc_pcg_normal(&r));
+            total += (double)(float)m;
+            mass[i] = (float)m;
+            orc_mixture_point(seed, cx, cy, sig, i, &pos[2 * i], &pos[2 * i + 1]);
+            vel[2 * i] = 0.0f;
+            vel[2 * i + 1] = 0.0f;
+        } else { /* projected Plummer sphere, a = 0.1 */
+            const double a = 0.1;
+            const double u = orc_pcg_uniform(&r) * 0.999;
+            const double R = a * sqrt(u / (1.0 - u));
+            const double angle = orc_pcg_uniform(&r) * 2.0 * ORC_PI;
+            const double x = R * cos(angle), y = R * sin(angle);
+            const double menc = R * R / (R * R + a * a);
+            const double Rs = R > 1e-9 ? R : 1e-9;
+            const double v = sqrt(G * menc / Rs);
+            orc_put(mass, pos, vel, i, 1.0 / (double)n, x, y, -v * (y / Rs), v * (x / Rs));
+        }
+    }
+    if (sc == 5 && total > 0.0)
+        for (uint32_t i = 0; i < n; ++i) mass[i] = (float)((double)mass[i] / total);
+    return 0;
+}

@@ -167,6 +167,13 @@ void orc_colormap(float t, float rgb[3]);
 void orc_diagnostics_fp64(const orc_params* p, uint32_t n, const float* mass, const float* pos,
                           const float* vel, double out[8]);
 
+/* Scenarios with one PCG32 stream per body (the engine's GPU generators):
+ * body i draws from PCG32(seed, sequence splitmix64(i)); formulas of the
+ * engine's host generators (simulation.ts:233-374 and the benchmark
+ * scenarios).  Returns -1 for an unknown name.  radius may be NULL. */
+int orc_generate_per_body(const char* name, uint32_t n, uint64_t seed, double G, float* mass,
+                          float* pos, float* vel, float* radius);
+
 /* OpenMP thread count the parallel paths use. */
 int orc_max_threads(void);
 

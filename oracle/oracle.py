@@ -89,6 +89,8 @@ def load() -> ctypes.CDLL:
         "orc_tone_map": (None, [ctypes.c_uint32, _P, _P]),
         "orc_colormap": (None, [ctypes.c_float, _P]),
         "orc_diagnostics_fp64": (None, [P, ctypes.c_uint32, _P, _P, _P, _P]),
+        "orc_generate_per_body": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint64,
+                                                 ctypes.c_double, _P, _P, _P, _P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -242,6 +244,18 @@ def diagnostics_fp64(p: OrcParams, mass, pos, vel) -> dict:
                              _p(f32(vel, (-1, 2))), _p(out))
     return dict(total_mass=out[0], com=out[1:3], momentum=out[3:5], angular_momentum=out[5],
                 kinetic_energy=out[6], potential_energy=out[7])
+
+
+def generate_per_body(name: str, n: int, seed: int, G: float = 1.0):
+    """Scenario with one PCG32 stream per body: (mass, pos, vel, radius)."""
+    lib = load()
+    mass = np.zeros(n, np.float32)
+    pos = np.zeros((n, 2), np.float32)
+    vel = np.zeros((n, 2), np.float32)
+    rad = np.zeros(n, np.float32)
+    if lib.orc_generate_per_body(name.encode(), n, seed, G, _p(mass), _p(pos), _p(vel), _p(rad)):
+        raise ValueError(f"Unknown scenario: {name}")
+    return mass, pos, vel, rad
 
 
 def render_density(cam, width: int, height: int, pos, radius_multiplier) -> np.ndarray:

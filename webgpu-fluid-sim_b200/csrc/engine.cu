@@ -32,6 +32,7 @@ struct bh_sim {
     uint32_t n = 50000;  // simulation.ts:60
     std::string scenario = "default";
     uint64_t seed = 0;
+    bool device_gen = false;  // the scenario comes from the GPU generators
     DeviceBuffers b;
     void* arena = nullptr;
     size_t arena_bytes = 0;
@@ -622,7 +623,31 @@ extern "C" int bh_generate_scenario(const char* name, uint32_t n, uint64_t seed,
     return BH_OK;
 }
 
+namespace bh {
+int scenario_id(const char* name);
+cudaError_t launch_generate(int scenario, uint32_t n, uint64_t seed, float grav_constant,
+                            float* mass, float2* pos, float2* vel, float* radius, int device,
+                            cudaStream_t stream);
+}  // namespace bh
+
+// The scenario generated on the GPU (one PCG32 stream per body).
+static int load_scenario_device(bh_sim* s, const std::string& name, uint64_t seed, uint32_t n) {
+    const int id = bh::scenario_id(name.c_str());
+    if (id < 0) return fail(s, BH_ERR_UNKNOWN_SCENARIO, "Unknown scenario: " + name);
+    int rc = alloc_buffers(s, n);
+    if (rc != BH_OK) return rc;
+    s->scenario = name;
+    s->seed = seed;
+    s->n = n;
+    s->device_gen = true;
+    BH_CUDA(s, bh::launch_generate(id, n, seed, s->cfg.grav_constant, s->b.mass, s->b.pos,
+                                   s->b.vel, s->b.radius, s->device, s->stream));
+    BH_CUDA(s, cudaStreamSynchronize(s->stream));
+    return BH_OK;
+}
+
 static int load_scenario(bh_sim* s, const std::string& name, uint64_t seed, uint32_t n) {
+    if (s->device_gen) return load_scenario_device(s, name, seed, n);
     std::vector<float> mass(n), pos(2 * (size_t)n), vel(2 * (size_t)n), rad(n);
     if (bh::generate_scenario(name.c_str(), n, seed, s->cfg.grav_constant, mass.data(), pos.data(),
                               vel.data(), rad.data()) != 0)
@@ -656,7 +681,16 @@ extern "C" int bh_set_scenario(bh_sim* s, const char* name, uint64_t seed) {
     if (!name) return fail(s, BH_ERR_INVALID_ARGUMENT, "null scenario name");
     if (!s->sys_sizes.empty())
         return fail(s, BH_ERR_NOT_SUPPORTED, "use bh_ensemble_set_scenarios on an ensemble");
+    s->device_gen = false;
     return load_scenario(s, name, seed, s->n);
+}
+
+extern "C" int bh_set_scenario_device(bh_sim* s, const char* name, uint64_t seed) {
+    BH_HANDLE(s);
+    if (!name) return fail(s, BH_ERR_INVALID_ARGUMENT, "null scenario name");
+    if (!s->sys_sizes.empty())
+        return fail(s, BH_ERR_NOT_SUPPORTED, "use bh_ensemble_set_scenarios on an ensemble");
+    return load_scenario_device(s, name, seed, s->n);
 }
 
 // ---- ensembles (extension) ------------------------------------------------------

@@ -117,6 +117,17 @@ class Simulation:
         self._check(st)
         self.currentScenario = scenario
 
+    def setScenarioOnDevice(self, scenario: str, seed: int | None = None) -> None:
+        """setScenario with the bodies generated on the GPU (one PCG32 stream
+        per body; same distributions, a different sample than setScenario)."""
+        if seed is not None:
+            self.seed = int(seed)
+        st = self._lib.bh_set_scenario_device(self._h, scenario.encode(), self.seed)
+        if st == _lib.BH_ERR_UNKNOWN_SCENARIO:
+            raise _lib.BhError(st, f"Unknown scenario: {scenario}")
+        self._check(st)
+        self.currentScenario = scenario
+
     def getCommands(self, frames: int = 1) -> CommandBuffer:
         """simulation.ts:386-425: one frame = config.substeps steps."""
         return CommandBuffer(self, frames)
