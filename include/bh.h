@@ -256,6 +256,24 @@ int bh_rollout_grad(bh_sim* sim, uint32_t steps, uint32_t checkpoint_every,
                     const float* target_pos, float* loss, float* grad_pos, float* grad_vel,
                     float* grad_mass);
 
+/* ---- one system on several GPUs (extension; the reference has one device) */
+/* Every rank holds the whole state and builds the same tree (the pipeline is
+ * deterministic).  bh_set_walk_slots(lo, hi) makes each step integrate only
+ * the groups whose first sorted slot lies in [lo, hi) -- the ranks take
+ * consecutive ranges of [0, n) -- while force evaluations stay complete.
+ * After a step, bh_shard_pack writes what this rank updated -- (pos, vel)
+ * for symplectic Euler, (vel, acc) for leapfrog -- in sorted-slot order into
+ * a device chunk of 16 + 16 * capacity bytes (header {first slot, count, 0,
+ * 0}, then one float4 per body; capacity >= ceil(n / ranks) + 32 *
+ * bodies_per_lane covers any range); the caller all-gathers the chunks
+ * (NCCL) and bh_shard_unpack applies all of them, after which every rank
+ * holds the state one GPU would have computed.  Both are enqueued on the
+ * handle's stream.  Group walk only; not for ensembles (shard those by
+ * systems). */
+int bh_set_walk_slots(bh_sim* sim, uint32_t slot_lo, uint32_t slot_hi);
+int bh_shard_pack(bh_sim* sim, void* chunk, uint32_t capacity);
+int bh_shard_unpack(bh_sim* sim, const void* chunks, uint32_t num_chunks, uint32_t capacity);
+
 /* ---- batched ensembles (extension; no reference counterpart) ------------- */
 /* An ensemble handle advances many independent systems with one launch per
  * stage: the bodies of all systems are concatenated (system k owns bodies

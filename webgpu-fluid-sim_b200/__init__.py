@@ -9,5 +9,7 @@ from ._lib import BhError, load  # noqa: F401
 from .config import WORKLOADS, Config, getDefaultConfig  # noqa: F401
 from .render import RenderCommand, Renderer  # noqa: F401
 from .runlog import RunLog  # noqa: F401
+from .shard import (ShardedSimulation, all_gather_chunks, chunk_bytes,  # noqa: F401
+                    chunk_capacity, partition_systems, slot_ranges)
 from .simulation import (SCENARIOS, CommandBuffer, Ensemble, SimBuffers,  # noqa: F401
                          Simulation, ensemble_sizes, generate_scenario, submit)

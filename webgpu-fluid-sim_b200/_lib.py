@@ -142,6 +142,9 @@ SIGNATURES = {
     "bh_set_scenario_device": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_uint64]),
     "bh_generate_scenario_device": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint64,
                                                    ctypes.c_float, _P, _P, _P, _P, _P]),
+    "bh_set_walk_slots": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32]),
+    "bh_shard_pack": (ctypes.c_int, [_P, _P, ctypes.c_uint32]),
+    "bh_shard_unpack": (ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint32]),
     "bh_diagnostics_compute": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(bh_diagnostics)]),
     "bh_renderer_create": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_P)]),
     "bh_renderer_destroy": (ctypes.c_int, [_P]),

@@ -77,6 +77,7 @@ constexpr int kGroupDfsAt = kGroupStack - 128;  // switch to one node per step a
 constexpr int kGroupList = 64;
 constexpr int kGroupMaxLeaf = 8;                // leaf_size cap of the group walk
 constexpr uint32_t kErrGroupStack = 1u << 3;    // group-walk stack overflow (never expected)
+constexpr uint32_t kErrShardCapacity = 1u << 4; // a shard's updated range exceeded its chunk
 
 // Walk modes.
 enum WalkMode : int {
@@ -105,6 +106,9 @@ struct WalkParams {
     // ensemble: a group only sees its own system's slot range
     uint32_t num_systems;
     const uint32_t* sys_off;
+    // sharding: only groups whose first sorted slot lies in [slot_lo, slot_hi)
+    uint32_t slot_lo;
+    uint32_t slot_hi;
 };
 
 // Per-step scratch that must start at zero.  One memset clears it.
@@ -115,6 +119,7 @@ struct StepScratch {
     unsigned long long walk_counts[4];  // instrumented walk counters
     unsigned int group_ctr[4];          // group walk: [0] work counter, [1] number of groups
     unsigned int frontier_ctr;          // hierarchy build: frontier nodes of the local phase
+    unsigned int shard_ma, shard_mb;    // sharding: n - (first / next group start), max-reduced
 };
 
 struct DeviceBuffers {
@@ -193,5 +198,10 @@ void init_bound(const DeviceBuffers& b, cudaStream_t s);
 void launch_walk(const DeviceBuffers& b, const WalkParams& p, int block, cudaStream_t s);
 // walk_group.cu
 void launch_walk_group(const DeviceBuffers& b, const WalkParams& p, int block, cudaStream_t s);
+// shard.cu: the bodies a sharded step updated, packed / unpacked in sorted-slot order
+void launch_shard_pack(const DeviceBuffers& b, uint32_t lo, uint32_t hi, int kdk, void* chunk,
+                       uint32_t capacity, cudaStream_t s);
+void launch_shard_unpack(const DeviceBuffers& b, int kdk, const void* chunks, uint32_t nchunks,
+                         uint32_t capacity, cudaStream_t s);
 
 }  // namespace bh

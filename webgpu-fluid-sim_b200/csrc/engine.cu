@@ -33,6 +33,8 @@ struct bh_sim {
     std::string scenario = "default";
     uint64_t seed = 0;
     bool device_gen = false;  // the scenario comes from the GPU generators
+    // sharding: the step's walk integrates only groups starting in these slots
+    uint32_t shard_lo = 0, shard_hi = 0xFFFFFFFFu;
     DeviceBuffers b;
     void* arena = nullptr;
     size_t arena_bytes = 0;
@@ -366,6 +368,11 @@ static bh::WalkParams walk_params(const bh_sim* s, int mode) {
     p.group_ctr = s->b.scratch ? s->b.scratch->group_ctr : nullptr;
     p.num_systems = s->b.num_systems;
     p.sys_off = s->b.sys_off;
+    // Sharding restricts the integrating walk of a step; force evaluations
+    // (the first leapfrog force, bh_compute_accelerations) cover every body.
+    const bool integrating = mode == bh::kWalkEulerKickDrift || mode == bh::kWalkKdkClose;
+    p.slot_lo = integrating ? s->shard_lo : 0u;
+    p.slot_hi = integrating ? s->shard_hi : 0xFFFFFFFFu;
     return p;
 }
 
@@ -485,6 +492,8 @@ static int check_device_errors(bh_sim* s) {
     if (e & bh::kErrLookbackSpin) msg += " sort look-back gave up waiting;";
     if (e & bh::kErrStackOverflow) msg += " walk stack full (children dropped);";
     if (e & bh::kErrTreeSpin) msg += " tree build gave up waiting;";
+    if (e & bh::kErrGroupStack) msg += " group-walk stack full;";
+    if (e & bh::kErrShardCapacity) msg += " shard chunk too small for its updated bodies;";
     // Restore the build's exchange slots so the next step starts clean.
     if (s->b.n > 1) BH_CUDA(s, cudaMemsetAsync(s->b.bound, 0xFF, sizeof(uint32_t) * (s->b.n - 1), s->stream));
     return fail(s, BH_ERR_DEVICE_CHECK, msg);
@@ -822,6 +831,39 @@ extern "C" int bh_step(bh_sim* s, uint32_t frames) {
         int rc = step_once(s);
         if (rc != BH_OK) return rc;
     }
+    return BH_OK;
+}
+
+// ---- sharding (extension) ---------------------------------------------------------
+
+extern "C" int bh_set_walk_slots(bh_sim* s, uint32_t slot_lo, uint32_t slot_hi) {
+    BH_HANDLE(s);
+    if (s->cfg.walk_mode != BH_WALK_GROUP)
+        return fail(s, BH_ERR_NOT_SUPPORTED, "sharded steps need the group walk");
+    if (s->b.num_systems > 0)
+        return fail(s, BH_ERR_NOT_SUPPORTED, "shard an ensemble by systems, not by slots");
+    if (slot_lo > slot_hi) return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_set_walk_slots: lo > hi");
+    s->shard_lo = slot_lo;
+    s->shard_hi = slot_hi;
+    destroy_graphs(s);  // captured steps carry the old walk parameters
+    return BH_OK;
+}
+
+extern "C" int bh_shard_pack(bh_sim* s, void* chunk, uint32_t capacity) {
+    BH_HANDLE(s);
+    if (!chunk) return fail(s, BH_ERR_INVALID_ARGUMENT, "null chunk");
+    const int kdk = s->cfg.integrator == BH_INTEGRATOR_LEAPFROG_KDK;
+    bh::launch_shard_pack(s->b, s->shard_lo, s->shard_hi, kdk, chunk, capacity, s->stream);
+    BH_CUDA(s, cudaGetLastError());
+    return BH_OK;
+}
+
+extern "C" int bh_shard_unpack(bh_sim* s, const void* chunks, uint32_t nchunks, uint32_t capacity) {
+    BH_HANDLE(s);
+    if (!chunks && nchunks) return fail(s, BH_ERR_INVALID_ARGUMENT, "null chunks");
+    const int kdk = s->cfg.integrator == BH_INTEGRATOR_LEAPFROG_KDK;
+    bh::launch_shard_unpack(s->b, kdk, chunks, nchunks, capacity, s->stream);
+    BH_CUDA(s, cudaGetLastError());
     return BH_OK;
 }
 

@@ -128,6 +128,7 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
         // A group is a subtree of <= 32 x BPL bodies: contiguous sorted slots
         // inside one Morton cell, so its box stays compact.
         const uint2 grp = __ldg(&groups[g]);
+        if (grp.x < P.slot_lo || grp.x >= P.slot_hi) continue;  // another shard's group
         const uint32_t base = grp.x, nvalid = grp.y;
         const int kmax = (int)((nvalid + 31u) / 32u);  // sub-slots in use (uniform)
         // Ensemble: the slot range of this group's system (systems stay
