@@ -26,6 +26,7 @@
 // ancestors n of body j these are polynomials in x_j whose coefficients are
 // ten path sums; vjp_push_kernel climbs each leaf's ancestors to form them.
 #include "bh_internal.cuh"
+#include "packed.cuh"
 
 namespace bh {
 
@@ -36,7 +37,10 @@ constexpr int kVjpSlots = 32 + 32 * kGroupMaxLeaf;
 
 struct VjpSmem {
     uint32_t stack[kVjpStack];
-    float4 nd[kGroupList][2];  // {cx, cy, m, node index bits}, {Q'xx, Q'xy, Q'yy, 0}
+    // node entry j, every value duplicated so a 64-bit shared load gives an
+    // operand pair: {cx, cx, cy, cy}, {m, m, Q'xx, Q'xx}, {Q'xy, Q'xy, Q'yy, Q'yy}
+    float4 nd[kGroupList][3];
+    uint32_t nd_idx[kGroupList];  // the entry's internal node
     uint32_t slot[kVjpSlots];
     float4 body[32];           // staged leaf records {x, y, m, slot bits}
 };
@@ -143,40 +147,115 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
             ghiy = fmaxf(ghiy, __shfl_xor_sync(FULL, ghiy, o));
         }
 
-        auto eval_nodes = [&](int cnt) {
-            for (int j = 0; j < cnt; ++j) {
-                const float4 mom = S.nd[j][0];
-                const uint32_t v = __float_as_uint(mom.w);
-                const float4 q4 = S.nd[j][1];
-                const float qxx = q4.x, qxy = q4.y, qyy = q4.z;
-                float cbx = 0.f, cby = 0.f, mb = 0.f, gxx = 0.f, gxy = 0.f, gyy = 0.f;
+        // Packed pairs of the lane's bodies (BPL >= 2): positions, adjoints
+        // and the node-list part of their position adjoints.
+        constexpr int NP = BPL / 2;
+        f2x PX[NP > 0 ? NP : 1], PY[NP > 0 ? NP : 1], PAX[NP > 0 ? NP : 1], PAY[NP > 0 ? NP : 1];
+        f2x PXB[NP > 0 ? NP : 1], PYB[NP > 0 ? NP : 1];
 #pragma unroll
-                for (int k = 0; k < BPL; ++k) {
-                    if (!ok[k]) continue;
-                    const float rx = mom.x - bx[k], ry = mom.y - by[k];
-                    const float s = rsqrt_ftz(fmaf(rx, rx, fmaf(ry, ry, eps2)));
-                    const float s2 = s * s, s3 = s * s2, s5 = s3 * s2;
-                    const float ar = abx[k] * rx + aby[k] * ry;
-                    float rbx = mom.z * (s3 * abx[k] - 3.0f * s5 * ar * rx);
-                    float rby = mom.z * (s3 * aby[k] - 3.0f * s5 * ar * ry);
-                    mb += ar * s3;
-                    if (MP >= 2) {
-                        const float s7 = s5 * s2, s9 = s7 * s2;
-                        const float qrx = qxx * rx + qxy * ry, qry = qxy * rx + qyy * ry;
-                        const float qax = qxx * abx[k] + qxy * aby[k], qay = qxy * abx[k] + qyy * aby[k];
-                        const float rqr = rx * qrx + ry * qry;
-                        const float aqr = abx[k] * qrx + aby[k] * qry;
-                        const float c1 = 5.0f * s7 * aqr - 17.5f * s9 * rqr * ar;
-                        rbx += -s5 * qax + c1 * rx + 5.0f * s7 * ar * qrx + 2.5f * s7 * rqr * abx[k];
-                        rby += -s5 * qay + c1 * ry + 5.0f * s7 * ar * qry + 2.5f * s7 * rqr * aby[k];
-                        gxx += -abx[k] * rx * s5 + 2.5f * rx * rx * ar * s7;
-                        gxy += -(abx[k] * ry + aby[k] * rx) * s5 + 5.0f * rx * ry * ar * s7;
-                        gyy += -aby[k] * ry * s5 + 2.5f * ry * ry * ar * s7;
+        for (int q = 0; q < NP; ++q) {
+            PX[q] = pk(bx[2 * q], bx[2 * q + 1]);
+            PY[q] = pk(by[2 * q], by[2 * q + 1]);
+            PAX[q] = pk(abx[2 * q], abx[2 * q + 1]);
+            PAY[q] = pk(aby[2 * q], aby[2 * q + 1]);
+            PXB[q] = pk(0.f, 0.f);
+            PYB[q] = pk(0.f, 0.f);
+        }
+        const int kmax = (int)((nvalid + 31u) / 32u);  // sub-slots in use (uniform)
+
+        auto eval_nodes = [&](int cnt) {
+#pragma unroll 2
+            for (int j = 0; j < cnt; ++j) {
+                const float4 e0 = S.nd[j][0], e1 = S.nd[j][1], e2 = S.nd[j][2];
+                const uint32_t v = S.nd_idx[j];
+                float cbx = 0.f, cby = 0.f, mb = 0.f, gxx = 0.f, gxy = 0.f, gyy = 0.f;
+                if (NP > 0) {
+                    // Two bodies per instruction.  A slot past the group's end
+                    // holds a zero adjoint, so it adds exactly zero everywhere.
+                    const f2x CX = ld_pair(e0, 0), CY = ld_pair(e0, 1), M = ld_pair(e1, 0);
+                    const f2x QXX = ld_pair(e1, 1), QXY = ld_pair(e2, 0), QYY = ld_pair(e2, 1);
+                    const f2x E2 = pk(eps2, eps2), CM3 = pk(-3.0f, -3.0f), CM1 = pk(-1.0f, -1.0f);
+                    const f2x C5 = pk(5.0f, 5.0f), C25 = pk(2.5f, 2.5f), CM175 = pk(-17.5f, -17.5f);
+                    f2x CB_X = pk(0.f, 0.f), CB_Y = CB_X, MB = CB_X, GXX = CB_X, GXY = CB_X, GYY = CB_X;
+#pragma unroll
+                    for (int q = 0; q < NP; ++q) {
+                        if (2 * q >= kmax) break;
+                        const f2x rx = sub2(CX, PX[q]), ry = sub2(CY, PY[q]);
+                        const f2x sv = rsqrt2(fma2(rx, rx, fma2(ry, ry, E2)));
+                        const f2x s2 = mul2(sv, sv), s3 = mul2(sv, s2), s5 = mul2(s3, s2);
+                        const f2x ar = fma2(PAX[q], rx, mul2(PAY[q], ry));
+                        const f2x tn = mul2(mul2(s5, ar), CM3);  // -3 s^5 (ab.r)
+                        f2x rbx = mul2(M, fma2(s3, PAX[q], mul2(tn, rx)));
+                        f2x rby = mul2(M, fma2(s3, PAY[q], mul2(tn, ry)));
+                        MB = fma2(ar, s3, MB);
+                        if (MP >= 2) {
+                            const f2x s7 = mul2(s5, s2), s9 = mul2(s7, s2), s5n = mul2(s5, CM1);
+                            const f2x qrx = fma2(QXX, rx, mul2(QXY, ry));
+                            const f2x qry = fma2(QXY, rx, mul2(QYY, ry));
+                            const f2x qax = fma2(QXX, PAX[q], mul2(QXY, PAY[q]));
+                            const f2x qay = fma2(QXY, PAX[q], mul2(QYY, PAY[q]));
+                            const f2x rqr = fma2(rx, qrx, mul2(ry, qry));
+                            const f2x aqr = fma2(PAX[q], qrx, mul2(PAY[q], qry));
+                            const f2x f7 = mul2(C5, s7), h7 = mul2(C25, s7);
+                            const f2x c1 = fma2(f7, aqr, mul2(mul2(CM175, s9), mul2(rqr, ar)));
+                            const f2x f7ar = mul2(f7, ar), h7ar = mul2(h7, ar), h7rqr = mul2(h7, rqr);
+                            rbx = fma2(s5n, qax, rbx);
+                            rbx = fma2(c1, rx, rbx);
+                            rbx = fma2(f7ar, qrx, rbx);
+                            rbx = fma2(h7rqr, PAX[q], rbx);
+                            rby = fma2(s5n, qay, rby);
+                            rby = fma2(c1, ry, rby);
+                            rby = fma2(f7ar, qry, rby);
+                            rby = fma2(h7rqr, PAY[q], rby);
+                            GXX = fma2(mul2(PAX[q], rx), s5n, fma2(mul2(rx, rx), h7ar, GXX));
+                            GXY = fma2(fma2(PAX[q], ry, mul2(PAY[q], rx)), s5n,
+                                       fma2(mul2(rx, ry), f7ar, GXY));
+                            GYY = fma2(mul2(PAY[q], ry), s5n, fma2(mul2(ry, ry), h7ar, GYY));
+                        }
+                        PXB[q] = sub2(PXB[q], rbx);
+                        PYB[q] = sub2(PYB[q], rby);
+                        CB_X = add2(CB_X, rbx);
+                        CB_Y = add2(CB_Y, rby);
                     }
-                    xbx[k] -= rbx;
-                    xby[k] -= rby;
-                    cbx += rbx;
-                    cby += rby;
+                    cbx = sum_halves(CB_X);
+                    cby = sum_halves(CB_Y);
+                    mb = sum_halves(MB);
+                    if (MP >= 2) {
+                        gxx = sum_halves(GXX);
+                        gxy = sum_halves(GXY);
+                        gyy = sum_halves(GYY);
+                    }
+                } else {
+                    const float cxn = e0.x, cyn = e0.z, mn = e1.x;
+                    const float qxx = e1.z, qxy = e2.x, qyy = e2.z;
+#pragma unroll
+                    for (int k = 0; k < BPL; ++k) {
+                        if (!ok[k]) continue;
+                        const float rx = cxn - bx[k], ry = cyn - by[k];
+                        const float s = rsqrt_ftz(fmaf(rx, rx, fmaf(ry, ry, eps2)));
+                        const float s2 = s * s, s3 = s * s2, s5 = s3 * s2;
+                        const float ar = abx[k] * rx + aby[k] * ry;
+                        float rbx = mn * (s3 * abx[k] - 3.0f * s5 * ar * rx);
+                        float rby = mn * (s3 * aby[k] - 3.0f * s5 * ar * ry);
+                        mb += ar * s3;
+                        if (MP >= 2) {
+                            const float s7 = s5 * s2, s9 = s7 * s2;
+                            const float qrx = qxx * rx + qxy * ry, qry = qxy * rx + qyy * ry;
+                            const float qax = qxx * abx[k] + qxy * aby[k], qay = qxy * abx[k] + qyy * aby[k];
+                            const float rqr = rx * qrx + ry * qry;
+                            const float aqr = abx[k] * qrx + aby[k] * qry;
+                            const float c1 = 5.0f * s7 * aqr - 17.5f * s9 * rqr * ar;
+                            rbx += -s5 * qax + c1 * rx + 5.0f * s7 * ar * qrx + 2.5f * s7 * rqr * abx[k];
+                            rby += -s5 * qay + c1 * ry + 5.0f * s7 * ar * qry + 2.5f * s7 * rqr * aby[k];
+                            gxx += -abx[k] * rx * s5 + 2.5f * rx * rx * ar * s7;
+                            gxy += -(abx[k] * ry + aby[k] * rx) * s5 + 5.0f * rx * ry * ar * s7;
+                            gyy += -aby[k] * ry * s5 + 2.5f * ry * ry * ar * s7;
+                        }
+                        xbx[k] -= rbx;
+                        xby[k] -= rby;
+                        cbx += rbx;
+                        cby += rby;
+                    }
                 }
                 if (MP >= 2) {
                     float vals[8] = {cbx, cby, mb, gxx, gxy, gyy, 0.f, 0.f};
@@ -274,9 +353,12 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
             const unsigned mn = __ballot_sync(FULL, emit_node);
             if (emit_node) {
                 const int p = nn + __popc(mn & lt);
-                S.nd[p][0] = make_float4(mom.x, mom.y, mom.z, __uint_as_float(v));
                 const float tr = sq.x + sq.z;  // Q' = 3S - tr(S) I
-                S.nd[p][1] = make_float4(3.0f * sq.x - tr, 3.0f * sq.y, 3.0f * sq.z - tr, 0.0f);
+                const float qxx = 3.0f * sq.x - tr, qxy = 3.0f * sq.y, qyy = 3.0f * sq.z - tr;
+                S.nd[p][0] = make_float4(mom.x, mom.x, mom.y, mom.y);
+                S.nd[p][1] = make_float4(mom.z, mom.z, qxx, qxx);
+                S.nd[p][2] = make_float4(qxy, qxy, qyy, qyy);
+                S.nd_idx[p] = v;
             }
             nn += __popc(mn);
             {
@@ -319,6 +401,16 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
         if (nn > 0) eval_nodes(nn);
         if (ns > 0) eval_bodies(ns);
         __syncwarp();
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {  // node-list part of the packed bodies
+            float lo, hi;
+            upk(PXB[q], lo, hi);
+            xbx[2 * q] += lo;
+            xbx[2 * q + 1] += hi;
+            upk(PYB[q], lo, hi);
+            xby[2 * q] += lo;
+            xby[2 * q + 1] += hi;
+        }
 #pragma unroll
         for (int k = 0; k < BPL; ++k) {
             if (!ok[k]) continue;

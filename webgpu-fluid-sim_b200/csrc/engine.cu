@@ -1031,13 +1031,24 @@ extern "C" int bh_rollout_grad(bh_sim* s, uint32_t steps, uint32_t checkpoint_ev
     const size_t vb = 8 * (size_t)n;
     const float dt = s->cfg.delta_time, h = 0.5f * dt;
     BH_CUDA(s, cudaMemcpyAsync(a.target, target_pos, vb, cudaMemcpyHostToDevice, st));
-    // Forward: T steps, saving (x, v) at every checkpoint.
+    // Forward: T steps, saving (x, v) at every checkpoint.  The last segment
+    // is recorded as its replay would record it (positions per step, trees in
+    // the slab): a replayed step reproduces the forward step bit for bit (same
+    // inputs, same deterministic pipeline), so that segment needs no replay.
+    const uint32_t c_last = (nck - 1) * K;
+    const bool last_saved = a.slab && a.slab_steps >= steps - c_last;
     for (uint32_t k = 0; k < steps; ++k) {
         if (k % K == 0) {
             BH_CUDA(s, cudaMemcpyAsync(a.ck_pos + (size_t)(k / K) * n, s->b.pos, vb, cudaMemcpyDeviceToDevice, st));
             BH_CUDA(s, cudaMemcpyAsync(a.ck_vel + (size_t)(k / K) * n, s->b.vel, vb, cudaMemcpyDeviceToDevice, st));
         }
+        if (k == c_last) BH_CUDA(s, cudaMemcpyAsync(a.seg_pos, s->b.pos, vb, cudaMemcpyDeviceToDevice, st));
         if ((rc = step_once(s)) != BH_OK) return rc;
+        if (k >= c_last) {
+            BH_CUDA(s, cudaMemcpyAsync(a.seg_pos + (size_t)(k + 1 - c_last) * n, s->b.pos, vb,
+                                       cudaMemcpyDeviceToDevice, st));
+            if (last_saved && (rc = save_tree(s, k - c_last)) != BH_OK) return rc;
+        }
     }
     BH_CUDA(s, cudaMemcpyAsync(a.fin_pos, s->b.pos, vb, cudaMemcpyDeviceToDevice, st));
     BH_CUDA(s, cudaMemcpyAsync(a.fin_vel, s->b.vel, vb, cudaMemcpyDeviceToDevice, st));
@@ -1046,17 +1057,19 @@ extern "C" int bh_rollout_grad(bh_sim* s, uint32_t steps, uint32_t checkpoint_ev
     // Reverse sweep, one checkpoint segment at a time (replay rebuilds the trees).
     for (int64_t seg = (int64_t)nck - 1; seg >= 0; --seg) {
         const uint32_t c = (uint32_t)seg * K, e = (c + K < steps) ? c + K : steps;
-        BH_CUDA(s, cudaMemcpyAsync(s->b.pos, a.ck_pos + (size_t)seg * n, vb, cudaMemcpyDeviceToDevice, st));
-        BH_CUDA(s, cudaMemcpyAsync(s->b.vel, a.ck_vel + (size_t)seg * n, vb, cudaMemcpyDeviceToDevice, st));
-        s->acc_valid = false;
-        BH_CUDA(s, cudaMemcpyAsync(a.seg_pos, s->b.pos, vb, cudaMemcpyDeviceToDevice, st));
         const bool saved = a.slab && a.slab_steps >= e - c;
-        for (uint32_t k = c; k < e; ++k) {
-            if ((rc = step_once(s)) != BH_OK) return rc;
-            BH_CUDA(s, cudaMemcpyAsync(a.seg_pos + (size_t)(k + 1 - c) * n, s->b.pos, vb,
-                                       cudaMemcpyDeviceToDevice, st));
-            // the step's tree is the one at x_{k+1}, where its reverse step needs the VJP
-            if (saved && (rc = save_tree(s, k - c)) != BH_OK) return rc;
+        if (c != c_last) {  // the last segment was recorded by the forward pass
+            BH_CUDA(s, cudaMemcpyAsync(s->b.pos, a.ck_pos + (size_t)seg * n, vb, cudaMemcpyDeviceToDevice, st));
+            BH_CUDA(s, cudaMemcpyAsync(s->b.vel, a.ck_vel + (size_t)seg * n, vb, cudaMemcpyDeviceToDevice, st));
+            s->acc_valid = false;
+            BH_CUDA(s, cudaMemcpyAsync(a.seg_pos, s->b.pos, vb, cudaMemcpyDeviceToDevice, st));
+            for (uint32_t k = c; k < e; ++k) {
+                if ((rc = step_once(s)) != BH_OK) return rc;
+                BH_CUDA(s, cudaMemcpyAsync(a.seg_pos + (size_t)(k + 1 - c) * n, s->b.pos, vb,
+                                           cudaMemcpyDeviceToDevice, st));
+                // the step's tree is the one at x_{k+1}, where its reverse step needs the VJP
+                if (saved && (rc = save_tree(s, k - c)) != BH_OK) return rc;
+            }
         }
         for (int64_t k = (int64_t)e - 1; k >= (int64_t)c; --k) {
             // closing kick of step k (force at x_{k+1}) plus the pending opening

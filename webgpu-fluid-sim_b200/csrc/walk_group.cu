@@ -42,6 +42,7 @@
 // accumulation is a plain fused multiply-add.  With eps^2 > 0 a body's own
 // leaf adds exactly zero (r = 0), so no self test is needed.
 #include "bh_internal.cuh"
+#include "packed.cuh"
 
 namespace bh {
 
@@ -60,47 +61,13 @@ struct GroupSmem {
     float4 body[32][2];        // 32 staged leaf records as pairs {x,x,y,y}, {m,m,0,0}
 };
 
-// ---- packed FP32 pairs (sm_100 .f32x2) ----------------------------------------
-typedef unsigned long long f2x;
-__device__ __forceinline__ f2x pk(float lo, float hi) {
-    f2x r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-__device__ __forceinline__ void upk(f2x v, float& lo, float& hi) {
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ f2x sub2(f2x a, f2x b) {
-    f2x r;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ f2x mul2(f2x a, f2x b) {
-    f2x r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ f2x fma2(f2x a, f2x b, f2x c) {
-    f2x r;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-    return r;
-}
-__device__ __forceinline__ f2x rsqrt2(f2x v) {
-    float lo, hi;
-    upk(v, lo, hi);
-    return pk(rsqrt_ftz(lo), rsqrt_ftz(hi));
-}
-__device__ __forceinline__ f2x ld_pair(const float4& v, int half) {
-    // {v.x, v.y} or {v.z, v.w} of a shared-memory float4 as one 64-bit pair
-    return reinterpret_cast<const f2x*>(&v)[half];
-}
-
-#ifndef BH_WALK_MIN_BLOCKS
-#define BH_WALK_MIN_BLOCKS 6  // resident blocks per SM the register budget is sized for (measured best)
-#endif
+// Resident blocks per SM the register budget is sized for (measured best:
+// 6 for groups of <= 64 bodies; 5 for 128-body groups, whose two packed
+// accumulator pairs per lane need more registers).
+constexpr int walk_min_blocks(int bpl) { return bpl >= 4 ? 5 : 6; }
 
 template <int BPL, int MP, bool PLUMMER>
-__global__ void __launch_bounds__(kGroupWarps * 32, BH_WALK_MIN_BLOCKS)
+__global__ void __launch_bounds__(kGroupWarps * 32, walk_min_blocks(BPL))
 walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ node4,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ ids,
                   float2* __restrict__ pos, float2* __restrict__ vel, float2* __restrict__ acc,
@@ -183,7 +150,7 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
 
         // Node list: multipole interactions.
         auto eval_nodes = [&](int cnt) {
-#pragma unroll 2
+#pragma unroll 4  // four independent entries in flight per lane (measured best)
             for (int j = 0; j < cnt; ++j) {
                 const float4 e0 = S.ent[j][0], e1 = S.ent[j][1];
                 float4 e2 = make_float4(0.f, 0.f, 0.f, 0.f);
