@@ -1,9 +1,10 @@
 """Benchmark: Barnes-Hut body-steps/s on the seeded colliding-disks workload.
 
 Workload (default): N = 800,000 bodies, two colliding exponential disks,
-theta = 0.5, Plummer eps = 1e-3, dt = 5e-5, leapfrog, 32-bit Morton keys over
-the bounding box.  One "step" = one full pipeline pass (kick-drift, Morton,
-sort, build + fill, walk + kick) over all bodies.
+theta = 0.5, Plummer eps = 1e-3, dt = 5e-5, the reference's symplectic Euler
+integrator, 32-bit Morton keys over the bounding box.  One "step" = one full
+pipeline pass (Morton, sort, build + fill, walk + kick + drift) over all
+bodies.
 
 Own arm (default):
   value      body-steps/s with the state resident in HBM, K steps timed with
