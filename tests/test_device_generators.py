@@ -99,3 +99,17 @@ def test_device_generator_raw_entry_and_errors(bh, orc):
     with pytest.raises(bh.BhError, match="Unknown scenario: nope"):
         sim.setScenarioOnDevice("nope")
     sim.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 2, 3, 7])
+def test_device_generator_tiny_counts(bh, orc, n):
+    for name in NAMES:
+        sim = bh.Simulation(bh.Config())
+        sim.setNumBodies(n)
+        sim.setScenarioOnDevice(name, 4)
+        mass, pos, vel = sim.download()
+        rm, rp, rv, _ = orc.generate_per_body(name, n, 4)
+        assert ulps(pos, rp).max() <= 1 and ulps(vel, rv).max() <= 1
+        assert ulps(mass, rm).max() <= 2
+        sim.close()

@@ -99,3 +99,18 @@ def test_run_log_entries(bh):
             assert k in e
     assert lines[0]["energy_drift"] == 0.0
     sim.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [0, 1, 2])
+def test_diagnostics_tiny_counts(bh, orc, n):
+    sim = bh.Simulation(bh.Config(softening="plummer", plummerEps=1e-2))
+    sim.setNumBodies(n)
+    d = sim.diagnostics()
+    assert d["pairs"] == n * (n - 1) // 2
+    if n == 0:
+        assert d["total_mass"] == 0.0 and d["potential_energy"] == 0.0
+    else:
+        mass, pos, vel = sim.download()
+        _check(d, orc.diagnostics_fp64(orc.params_from_config(sim.config), mass, pos, vel))
+    sim.close()

@@ -177,3 +177,19 @@ def test_render_skips_offscreen_and_non_finite_bodies(bh, orc):
     assert dens[8, 8] == pytest.approx(0.02 / 1.5, rel=1e-6)
     r.close()
     sim.close()
+
+
+@pytest.mark.gpu
+def test_render_with_no_bodies_and_one_pixel_canvas(bh):
+    sim = bh.Simulation(bh.Config())
+    sim.setNumBodies(0)
+    r, dens, img = _frame(bh, sim, 8, 4)
+    assert (dens == 0).all() and (img[:, :, :3] == 0).all() and (img[:, :, 3] == 255).all()
+    r.close()
+    sim.setNumBodies(10)
+    r, dens, img = _frame(bh, sim, 1, 1)
+    assert dens.shape == (1, 1) and np.isfinite(dens).all()
+    r.close()
+    with pytest.raises(bh.BhError):
+        bh.Renderer(sim, 0, 10)
+    sim.close()

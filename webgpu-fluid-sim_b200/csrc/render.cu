@@ -49,7 +49,13 @@ struct RenderParams {
 constexpr int kSplatThreads = 256;
 constexpr int kToneThreads = 256;
 
-// density.wgsl:39-97, one warp per 32 bodies.
+// density.wgsl:39-97, one warp per 32 bodies.  Each lane sets up its own
+// body once (centre and radius in pixels, pixel bounds, weight) and the warp
+// then splats the 32 bodies one after the other, the setup of each shuffled
+// from its lane.  The lanes cover the body's pixel rectangle in 8 x 4 tiles,
+// with integer pixel indices and exactly representable float pixel centres
+// stepped by additions: no division or conversion per pixel, one hardware
+// exponential per covered pixel.
 __global__ void __launch_bounds__(kSplatThreads)
 splat_kernel(const float2* __restrict__ pos, const float* __restrict__ radius_mul, uint32_t n,
              const RenderParams P, float* __restrict__ density) {
@@ -61,51 +67,58 @@ splat_kernel(const float2* __restrict__ pos, const float* __restrict__ radius_mu
     // zoom compensation (density.wgsl:86-88)
     const float zoom = fmaxf(P.hx, P.hy);
     const float zoom_scale = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(0.05f, zoom)));
+    const int tx = lane & 7, ty = lane >> 3;  // the lane's place in an 8 x 4 tile
     for (uint32_t base = warp * 32u; base < n; base += nwarps * 32u) {
-        float bx = 0.0f, by = 0.0f, bm = 0.0f;
+        // ---- this lane's body ----
+        float cpx = 0.0f, cpy = 0.0f, inv_r = 0.0f, bw = 0.0f;
+        int ia = 0, ib = -1, ja = 0, jb = -1;  // pixel rectangle [ia, ib] x [ja, jb]
         if (base + (uint32_t)lane < n) {
             const float2 p = __ldg(&pos[base + lane]);
-            bx = p.x;
-            by = p.y;
-            bm = __ldg(&radius_mul[base + lane]);
+            const float rm = __ldg(&radius_mul[base + lane]);
+            // vertex stage (density.wgsl:60-70): centre in NDC, radius in pixels
+            const float cnx = __fdiv_rn(__fsub_rn(p.x, P.cx), P.hx);
+            const float cny = __fdiv_rn(__fsub_rn(p.y, P.cy), P.hy);
+            const float R = __fmul_rn(2.0f, rm);
+            // centre in display pixel coordinates: (ndc + 1) / 2 * size
+            cpx = __fmul_rn(__fmul_rn(__fadd_rn(cnx, 1.0f), 0.5f), W);
+            cpy = __fmul_rn(__fmul_rn(__fadd_rn(cny, 1.0f), 0.5f), H);
+            // a body without a finite centre or radius draws nothing (the
+            // rasteriser drops a quad with non-finite vertices)
+            if (isfinite(cpx) && isfinite(cpy) && R > 0.0f && isfinite(R)) {
+                // pixel centres i + 1/2 within [c - R, c + R], clipped to the canvas
+                const float i0 = fmaxf(ceilf(cpx - R - 0.5f), 0.0f);
+                const float i1 = fminf(floorf(cpx + R - 0.5f), W - 1.0f);
+                const float j0 = fmaxf(ceilf(cpy - R - 0.5f), 0.0f);
+                const float j1 = fminf(floorf(cpy + R - 0.5f), H - 1.0f);
+                if (i0 <= i1 && j0 <= j1) {
+                    ia = (int)i0; ib = (int)i1; ja = (int)j0; jb = (int)j1;
+                }
+            }
+            inv_r = __frcp_rn(R);
+            bw = __fmul_rn(rm > 1.0f ? 0.1f : 0.02f, zoom_scale);  // density.wgsl:90-95
         }
         const int cnt = (n - base) < 32u ? (int)(n - base) : 32;
         for (int k = 0; k < cnt; ++k) {
-            const float x = __shfl_sync(FULL, bx, k);
-            const float y = __shfl_sync(FULL, by, k);
-            const float rm = __shfl_sync(FULL, bm, k);
-            // vertex stage (density.wgsl:60-70): centre in NDC, radius in pixels
-            const float cnx = __fdiv_rn(__fsub_rn(x, P.cx), P.hx);
-            const float cny = __fdiv_rn(__fsub_rn(y, P.cy), P.hy);
-            const float R = __fmul_rn(2.0f, rm);
-            // centre in display pixel coordinates: (ndc + 1) / 2 * size
-            const float cpx = __fmul_rn(__fmul_rn(__fadd_rn(cnx, 1.0f), 0.5f), W);
-            const float cpy = __fmul_rn(__fmul_rn(__fadd_rn(cny, 1.0f), 0.5f), H);
-            // a body without a finite centre or radius draws nothing (the
-            // rasteriser drops a quad with non-finite vertices)
-            if (!isfinite(cpx) || !isfinite(cpy) || !(R > 0.0f) || !isfinite(R)) continue;
-            // pixel centres i + 1/2 within [c - R, c + R], clipped to the canvas
-            const float i0 = fmaxf(ceilf(cpx - R - 0.5f), 0.0f);
-            const float i1 = fminf(floorf(cpx + R - 0.5f), W - 1.0f);
-            const float j0 = fmaxf(ceilf(cpy - R - 0.5f), 0.0f);
-            const float j1 = fminf(floorf(cpy + R - 0.5f), H - 1.0f);
-            if (!(i0 <= i1) || !(j0 <= j1)) continue;
-            const uint32_t ia = (uint32_t)i0, ja = (uint32_t)j0;
-            const uint32_t fw = (uint32_t)i1 - ia + 1u, fh = (uint32_t)j1 - ja + 1u;
-            const uint32_t count = fw * fh;
-            const float bw = __fmul_rn(rm > 1.0f ? 0.1f : 0.02f, zoom_scale);  // density.wgsl:90-95
-            const float inv_r = __frcp_rn(R);
-            for (uint32_t q = (uint32_t)lane; q < count; q += 32u) {
-                const uint32_t j = ja + q / fw, i = ia + q % fw;
+            const int kia = __shfl_sync(FULL, ia, k), kib = __shfl_sync(FULL, ib, k);
+            const int kja = __shfl_sync(FULL, ja, k), kjb = __shfl_sync(FULL, jb, k);
+            if (kia > kib) continue;  // nothing on screen (uniform)
+            const float kcx = __shfl_sync(FULL, cpx, k), kcy = __shfl_sync(FULL, cpy, k);
+            const float kir = __shfl_sync(FULL, inv_r, k), kbw = __shfl_sync(FULL, bw, k);
+            float yc = (float)(kja + ty) + 0.5f;
+            for (int j = kja + ty; j <= kjb; j += 4, yc = __fadd_rn(yc, 4.0f)) {
                 // uv and r^2 = |uv|^2; discard outside the disc (density.wgsl:73-78)
-                const float ux = __fmul_rn(__fsub_rn((float)i + 0.5f, cpx), inv_r);
-                const float uy = __fmul_rn(__fsub_rn((float)j + 0.5f, cpy), inv_r);
-                const float r2 = __fadd_rn(__fmul_rn(ux, ux), __fmul_rn(uy, uy));
-                if (r2 > 1.0f) continue;
-                // w = exp(-k r^2), k = 10 (density.wgsl:81-82): the hardware
-                // exponential, relative error ~1e-6 over r^2 in [0, 1]
-                const float w = __expf(__fmul_rn(-10.0f, r2));
-                atomicAdd(&density[(size_t)j * P.w + i], __fmul_rn(bw, w));
+                const float uy = __fmul_rn(__fsub_rn(yc, kcy), kir);
+                const float uy2 = __fmul_rn(uy, uy);
+                float* row = density + (size_t)j * P.w;
+                float xc = (float)(kia + tx) + 0.5f;
+                for (int i = kia + tx; i <= kib; i += 8, xc = __fadd_rn(xc, 8.0f)) {
+                    const float ux = __fmul_rn(__fsub_rn(xc, kcx), kir);
+                    const float r2 = __fadd_rn(__fmul_rn(ux, ux), uy2);
+                    if (r2 > 1.0f) continue;
+                    // w = exp(-k r^2), k = 10 (density.wgsl:81-82): the hardware
+                    // exponential, relative error ~1e-6 over r^2 in [0, 1]
+                    atomicAdd(&row[i], __fmul_rn(kbw, __expf(__fmul_rn(-10.0f, r2))));
+                }
             }
         }
     }
