@@ -49,7 +49,7 @@ FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes (read + write) of one launch of the dominant kernel (the walk),
 # from one ncu capture of the same workload
 # (profiles/walk_group_build_fill_onesweep_colliding-disks-800k.md).
-NCU_WALK_TRAFFIC_BYTES = {"colliding-disks-800k": 52.32e6}
+NCU_WALK_TRAFFIC_BYTES = {"colliding-disks-800k": 44.16e6}
 
 
 def parse():

@@ -11,7 +11,10 @@
 // kernel lists the groups).  Fixed runs of G slots would not do: a run that
 // straddles a jump of the Z curve has a box spanning far-apart regions and
 // opens nearly every node.  (Cutting maximal 2G-body subtrees into G-slot
-// runs fills more lanes but opens more nodes; measured slower.)  The group
+// runs fills more lanes but opens more nodes; measured slower.  So did
+// stack entries that stand for both children of an opened node -- adjacent
+// in the Karras numbering, one round trip for the pair -- which halve the
+// dependent steps but double the emission work per step and the registers.)  The group
 // opens a node unless
 //     L^2 < theta^2 d^2,  L = longest side of the node's box,
 //     d = distance between the group's box and the node's box,
