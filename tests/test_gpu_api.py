@@ -1,0 +1,97 @@
+"""The reference's Simulation API semantics on the engine (simulation.ts).
+
+frames x substeps steps per submitted frame (simulation.ts:386-425), new
+buffers on every body-count or scenario change (:367-369), getBuffers() as
+borrowed device views, updateMetadataBuffer() without effect on results,
+host state round trips, and argument errors -- all through the C ABI.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _sim(bh, n=3000, **cfg):
+    s = bh.Simulation(bh.Config(**cfg))
+    s.setNumBodies(n)
+    s.setScenario("default", 12)
+    return s
+
+
+def test_frames_times_substeps(bh):
+    a = _sim(bh, substeps=3, deltaTime=1e-3)
+    b = _sim(bh, substeps=1, deltaTime=1e-3)
+    a.step(2)            # 2 frames x 3 substeps
+    b.step(6)
+    for x, y in zip(a.download(), b.download()):
+        assert np.array_equal(x, y)
+    a.close()
+    b.close()
+
+
+def test_submitted_commands_equal_step(bh):
+    a = _sim(bh)
+    b = _sim(bh)
+    bh.submit([a.getCommands(), a.getCommands()])  # main.ts:38-41
+    b.step(2)
+    for x, y in zip(a.download(), b.download()):
+        assert np.array_equal(x, y)
+    a.close()
+    b.close()
+
+
+def test_update_metadata_buffer_changes_nothing(bh):
+    a = _sim(bh)
+    b = _sim(bh)
+    a.updateMetadataBuffer()
+    a.step(3)
+    b.step(3)
+    for x, y in zip(a.download(), b.download()):
+        assert np.array_equal(x, y)
+    a.close()
+    b.close()
+
+
+def test_buffers_are_borrowed_views_renewed_on_change(bh):
+    s = _sim(bh, n=5000)
+    b1 = s.getBuffers()
+    assert b1.numBodies == 5000 and b1.pos and b1.mass and b1.stream
+    mass, pos, vel = s.download()
+    # the handle's device buffers hold the same data as the host copy
+    got = s.read_buffer("pos", np.float32, 2 * 5000).reshape(-1, 2)
+    assert np.array_equal(got, pos)
+    # a new body count reallocates (simulation.ts:367-369): new buffers, new size
+    s.setNumBodies(7000)
+    b2 = s.getBuffers()
+    assert b2.numBodies == 7000 and s.getNumBodies() == 7000
+    assert s.download()[1].shape == (7000, 2)
+    s.close()
+
+
+def test_upload_download_round_trip_and_errors(bh):
+    s = _sim(bh, n=1000)
+    rng = np.random.default_rng(3)
+    m = rng.random(1000, dtype=np.float32) + 0.5
+    p = rng.standard_normal((1000, 2)).astype(np.float32)
+    v = rng.standard_normal((1000, 2)).astype(np.float32)
+    s.upload(m, p, v)
+    m2, p2, v2 = s.download()
+    assert np.array_equal(m, m2) and np.array_equal(p, p2) and np.array_equal(v, v2)
+    s.upload(None, p * 2, None)  # NULL skips an array
+    m3, p3, v3 = s.download()
+    assert np.array_equal(m3, m) and np.array_equal(p3, p * 2) and np.array_equal(v3, v)
+    with pytest.raises(ValueError):
+        s.upload(m[:10], None, None)  # wrong length
+    with pytest.raises(ValueError):
+        s.setNumBodies(-1)
+    s.close()
+
+
+def test_zero_bodies_step_and_download(bh):
+    s = _sim(bh, n=0)
+    s.step(3)
+    s.sync()
+    m, p, v = s.download()
+    assert m.shape == (0,) and p.shape == (0, 2)
+    assert s.computeAccelerations().shape == (0, 2)
+    s.close()
