@@ -932,6 +932,15 @@ uint32_t orc_num_bodies(const orc_state* s) { return s->n; }
  * 1 / (1 + 0.05 max(half)) (:86-88), base 0.1 when rm > 1 else 0.02
  * (:90-93); evaluated as (base zoom_scale) exp(-10 |uv|^2) with uv scaled
  * by 1 / radius, as the CUDA kernel does. */
+float orc_splat_weight(float ux, float uy, float radius_multiplier, float zoom_scale,
+                       int* discarded) {
+    const float r2 = ux * ux + uy * uy;
+    *discarded = r2 > 1.0f;
+    if (*discarded) return 0.0f;
+    const float bw = (radius_multiplier > 1.0f ? 0.1f : 0.02f) * zoom_scale;
+    return bw * expf(-10.0f * r2);
+}
+
 void orc_render_density(const float cam[4], uint32_t width, uint32_t height, uint32_t n,
                         const float* pos, const float* radius_multiplier, double* density) {
     const float W = (float)width, H = (float)height;
@@ -953,15 +962,14 @@ void orc_render_density(const float cam[4], uint32_t width, uint32_t height, uin
         if (i1 > W - 1.0f) i1 = W - 1.0f;
         if (j1 > H - 1.0f) j1 = H - 1.0f;
         if (!(i0 <= i1) || !(j0 <= j1)) continue;
-        const float bw = (rm > 1.0f ? 0.1f : 0.02f) * zoom_scale;
         const float inv_r = 1.0f / R;
         for (uint32_t j = (uint32_t)j0; j <= (uint32_t)j1; ++j) {
             for (uint32_t i = (uint32_t)i0; i <= (uint32_t)i1; ++i) {
                 const float ux = (((float)i + 0.5f) - cpx) * inv_r;
                 const float uy = (((float)j + 0.5f) - cpy) * inv_r;
-                const float r2 = ux * ux + uy * uy;
-                if (r2 > 1.0f) continue;
-                density[(size_t)j * width + i] += (double)(bw * expf(-10.0f * r2));
+                int discarded;
+                const float w = orc_splat_weight(ux, uy, rm, zoom_scale, &discarded);
+                if (!discarded) density[(size_t)j * width + i] += (double)w;
             }
         }
     }
@@ -994,16 +1002,19 @@ static uint8_t orc_unorm8(float c) {
     return (uint8_t)lrintf(v);
 }
 
+void orc_tone_map_rgb(float texel, float rgb[3]) {
+    const float gamma = (float)(1.0 / 2.2);
+    const float x = 8.0f * texel;
+    const float mapped = x / (1.0f + x);
+    const float m = mapped < 0.0f ? 0.0f : (mapped > 1.0f ? 1.0f : mapped);
+    orc_colormap(powf(m, gamma), rgb);
+}
+
 /* tone_map.wgsl:63-84 (the r16float texel is the density rounded to FP16) */
 void orc_tone_map(uint32_t pixels, const float* density, uint8_t* rgba) {
-    const float gamma = (float)(1.0 / 2.2);
     for (uint32_t p = 0; p < pixels; ++p) {
-        const float d = (float)(_Float16)density[p];
-        const float x = 8.0f * d;
-        const float mapped = x / (1.0f + x);
-        const float m = mapped < 0.0f ? 0.0f : (mapped > 1.0f ? 1.0f : mapped);
         float rgb[3];
-        orc_colormap(powf(m, gamma), rgb);
+        orc_tone_map_rgb((float)(_Float16)density[p], rgb);
         rgba[4 * (size_t)p] = orc_unorm8(rgb[0]);
         rgba[4 * (size_t)p + 1] = orc_unorm8(rgb[1]);
         rgba[4 * (size_t)p + 2] = orc_unorm8(rgb[2]);

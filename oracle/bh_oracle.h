@@ -160,6 +160,13 @@ void orc_render_density(const float cam[4], uint32_t width, uint32_t height, uin
 void orc_tone_map(uint32_t pixels, const float* density, uint8_t* rgba);
 /* colormap(t) of tone_map.wgsl:24-46 (rgb). */
 void orc_colormap(float t, float rgb[3]);
+/* The per-pixel parts of the two passes: density.wgsl:73-97 for a pixel at
+ * quad coordinates (ux, uy) (discarded outside the disc), and
+ * tone_map.wgsl:63-84 for one r16float texel value (rgb before the unorm
+ * conversion). */
+float orc_splat_weight(float ux, float uy, float radius_multiplier, float zoom_scale,
+                       int* discarded);
+void orc_tone_map_rgb(float texel, float rgb[3]);
 
 /* FP64 diagnostics: out = {M, COM x, COM y, P x, P y, Lz, K, W}; W is the
  * direct pair sum -G sum_{i<j} m_i m_j / sqrt(r^2 + eps_ij^2) with the

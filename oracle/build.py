@@ -5,8 +5,9 @@
   written).  Tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
   ``bench.py`` load it; the engine never does.
 - ``oracle/_ref/``: a mechanical C++ translation of the reference's own WGSL
-  compute shaders, produced by ``wgsl_to_cpp.py`` from the shader files where
-  they lie in the reference checkout.  Built only where that checkout exists
+  compute shaders, and of the fragment stages of its render shaders, produced
+  by ``wgsl_to_cpp.py`` from the shader files where they lie in the
+  reference checkout.  Built only where that checkout exists
   (the build container); its outputs stay out of version control.
 """
 from __future__ import annotations
@@ -48,7 +49,11 @@ def build_ref(force: bool = False) -> str | None:
         return None
     sys.path.insert(0, HERE)
     import wgsl_to_cpp  # noqa: E402  (sibling module of this recipe)
-    return wgsl_to_cpp.build(shaders, REF_DIR, force=force)
+    lib = wgsl_to_cpp.build(shaders, REF_DIR, force=force)
+    render = os.path.join(REFERENCE_CHECKOUT, "src", "shaders", "render")
+    if os.path.isdir(render):
+        wgsl_to_cpp.build_render(render, REF_DIR, force=force)
+    return lib
 
 
 def build(force: bool = False) -> None:

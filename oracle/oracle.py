@@ -88,6 +88,9 @@ def load() -> ctypes.CDLL:
                                       _P]),
         "orc_tone_map": (None, [ctypes.c_uint32, _P, _P]),
         "orc_colormap": (None, [ctypes.c_float, _P]),
+        "orc_splat_weight": (ctypes.c_float, [ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                              ctypes.c_float, ctypes.POINTER(ctypes.c_int)]),
+        "orc_tone_map_rgb": (None, [ctypes.c_float, _P]),
         "orc_diagnostics_fp64": (None, [P, ctypes.c_uint32, _P, _P, _P, _P]),
         "orc_generate_per_body": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint64,
                                                  ctypes.c_double, _P, _P, _P, _P]),
@@ -276,6 +279,58 @@ def tone_map(density) -> np.ndarray:
     h, w = np.shape(density)
     out = np.zeros((h, w, 4), np.uint8)
     lib.orc_tone_map(h * w, _p(d), _p(out))
+    return out
+
+
+def splat_weight(ux: float, uy: float, radius_multiplier: float, zoom_scale: float):
+    """(density added, discarded) of one pixel at quad coordinates (ux, uy)."""
+    d = ctypes.c_int(0)
+    w = load().orc_splat_weight(ux, uy, radius_multiplier, zoom_scale, ctypes.byref(d))
+    return float(w), bool(d.value)
+
+
+def tone_map_rgb(texel: float) -> np.ndarray:
+    out = np.zeros(3, np.float32)
+    load().orc_tone_map_rgb(float(texel), _p(out))
+    return out
+
+
+REF_RENDER_LIB = os.path.join(HERE, "_ref", "libref_render.so")
+
+
+def ref_render_available() -> bool:
+    return os.path.exists(REF_RENDER_LIB)
+
+
+def _ref_render():
+    lib = ctypes.CDLL(REF_RENDER_LIB)
+    lib.ref_density_fragment.restype = ctypes.c_float
+    lib.ref_density_fragment.argtypes = [ctypes.c_float] * 5 + [ctypes.POINTER(ctypes.c_int)]
+    lib.ref_tone_map_fragment.restype = None
+    lib.ref_tone_map_fragment.argtypes = [ctypes.c_float, _P]
+    lib.ref_colormap.restype = None
+    lib.ref_colormap.argtypes = [ctypes.c_float, _P]
+    return lib
+
+
+def ref_density_fragment(ux, uy, radius_multiplier, half_x, half_y):
+    """The reference's translated density.wgsl fragment: (density, discarded)."""
+    d = ctypes.c_int(0)
+    w = _ref_render().ref_density_fragment(ux, uy, radius_multiplier, half_x, half_y,
+                                           ctypes.byref(d))
+    return float(w), bool(d.value)
+
+
+def ref_tone_map_fragment(texel: float) -> np.ndarray:
+    out = np.zeros(3, np.float32)
+    _ref_render().ref_tone_map_fragment(float(texel), _p(out))
+    return out
+
+
+def ref_colormap(t: float) -> np.ndarray:
+    """The reference's translated colormap (tone_map.wgsl:24-46)."""
+    out = np.zeros(3, np.float32)
+    _ref_render().ref_colormap(float(t), _p(out))
     return out
 
 

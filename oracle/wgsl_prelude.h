@@ -58,6 +58,35 @@ inline f32 dot(vec2f a, vec2f b) { return a.x * b.x + a.y * b.y; }
 inline f32 sqrt(f32 v) { return std::sqrt(v); }
 inline f32 inverseSqrt(f32 v) { return 1.0f / std::sqrt(v); }
 inline u32 atomicAdd(u32* p, u32 v) { u32 old = *p; *p = old + v; return old; }
+
+// ---- the render shaders' types and builtins (density.wgsl, tone_map.wgsl) ----
+struct vec3f {
+    f32 x = 0.0f, y = 0.0f, z = 0.0f;
+    vec3f() = default;
+    vec3f(f32 a, f32 b, f32 c) : x(a), y(b), z(c) {}
+};
+inline vec3f operator+(vec3f a, vec3f b) { return vec3f(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline vec3f operator*(vec3f a, f32 s) { return vec3f(a.x * s, a.y * s, a.z * s); }
+struct vec4f {
+    f32 x = 0.0f, y = 0.0f, z = 0.0f, w = 0.0f;
+    vec4f() = default;
+    vec4f(f32 a, f32 b, f32 c, f32 d) : x(a), y(b), z(c), w(d) {}
+    vec4f(vec2f a, f32 c, f32 d) : x(a.x), y(a.y), z(c), w(d) {}
+    vec4f(vec3f a, f32 d) : x(a.x), y(a.y), z(a.z), w(d) {}
+};
+inline f32 length(vec2f v) { return std::sqrt(dot(v, v)); }
+inline f32 exp(f32 v) { return std::exp(v); }
+inline f32 pow(f32 a, f32 b) { return std::pow(a, b); }
+// mix(e1, e2, t) = e1 * (1 - t) + e2 * t
+inline vec3f mix(vec3f a, vec3f b, f32 t) { return a * (1.0f - t) + b * t; }
+// A texture and a sampler: the harness sets the value a sample returns (the
+// tone map samples its density texture at texel centres, i.e. a texel).
+struct texture_2d {};
+struct sampler {};
+inline f32 g_texel = 0.0f;
+inline vec4f textureSample(texture_2d, sampler, vec2f) { return vec4f(g_texel, 0.0f, 0.0f, 1.0f); }
+// `discard` in a fragment shader: the harness reads this flag.
+inline bool g_discarded = false;
 inline void atomicStore(u32* p, u32 v) { *p = v; }
 
 }  // namespace wgsl

@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import os
 import re
+import struct
 import shutil
 import subprocess
 
@@ -32,6 +33,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 TYPE_MAP = {
     "f32": "f32", "u32": "u32", "i32": "i32", "bool": "bool",
     "vec2<f32>": "vec2f", "vec3<u32>": "vec3u", "atomic<u32>": "u32",
+    "vec3<f32>": "vec3f", "vec4<f32>": "vec4f",
 }
 
 
@@ -46,6 +48,8 @@ def ctype(t: str) -> str:
 
 def expr(s: str) -> str:
     s = s.replace("vec2<f32>(", "vec2f(").replace("vec3<u32>(", "vec3u(")
+    s = s.replace("vec3<f32>(", "vec3f(").replace("vec4<f32>(", "vec4f(")
+    s = s.replace(").r", ").x")  # the red channel of a sampled vec4
     # f32 literals (abstract floats concretised to f32 in these shaders)
     s = re.sub(r"(?<![\w.])(\d+\.\d*)(?![\w.])", r"\1f", s)
     return s
@@ -142,6 +146,82 @@ def translate(src: str, namespace: str) -> str:
         out.append(f"{ind}{expr(st)} {comment}".rstrip())
     out.append(f"}}  // namespace {namespace}")
     return "\n".join(out) + "\n"
+
+
+CONST_EXPR = re.compile(r"[0-9.\s+\-*/()]+")
+
+
+def translate_render(src: str, namespace: str) -> str:
+    """The render shaders (density.wgsl, tone_map.wgsl) without their vertex
+    stages: structs (attributes dropped), bindings (textures and samplers as
+    harness stubs), helper functions and the fragment entry point, whose
+    `discard` sets wgsl::g_discarded.  A `let` of literals alone is a WGSL
+    abstract-float constant expression: it is evaluated here in double
+    precision and stored as the nearest f32, as WGSL does."""
+    lines = []
+    skip = 0
+    it = iter(src.splitlines())
+    for raw in it:
+        st = split_comment(raw)[0].strip()
+        if st == "@vertex":  # drop the whole vertex entry point
+            depth = 0
+            for body in it:
+                code = split_comment(body)[0]
+                depth += code.count("{") - code.count("}")
+                if "{" in code and depth == 0:
+                    break
+                if depth == 0 and "}" in code:
+                    break
+            continue
+        if st == "@fragment":
+            lines.append("// @fragment")
+            continue
+        m = re.fullmatch(r"@group\(\d+\)\s*@binding\(\d+\)\s*var<storage,\s*read>\s+(\w+)\s*:\s*array<(.+)>\s*;", st)
+        if m:
+            lines.append(f"static {ctype(m.group(2))}* {m.group(1)} = nullptr;")
+            continue
+        m = re.fullmatch(r"@group\(\d+\)\s*@binding\(\d+\)\s*var\s+(\w+)\s*:\s*(texture_2d<f32>|sampler)\s*;", st)
+        if m:
+            ty = "texture_2d" if m.group(2).startswith("texture") else "sampler"
+            lines.append(f"static {ty} {m.group(1)};")
+            continue
+        m = re.fullmatch(r"let\s+(\w+)\s*=\s*(.+);", st)
+        if m and CONST_EXPR.fullmatch(m.group(2)):
+            ind = raw[: len(raw) - len(raw.lstrip())]
+            val = eval(m.group(2), {"__builtins__": {}})  # digits and + - * / ( ) only
+            f32 = struct.unpack("f", struct.pack("f", float(val)))[0]  # nearest f32
+            lines.append(f"{ind}const f32 {m.group(1)} = {f32!r};")
+            continue
+        raw = re.sub(r"@(builtin|location|interpolate)\([^)]*\)\s*", "", raw)
+        raw = raw.replace("discard;", "{ g_discarded = true; return {}; }")
+        lines.append(raw)
+    return translate("\n".join(lines), namespace)
+
+
+def build_render(shader_dir: str, out_dir: str, force: bool = False) -> str:
+    """Translate density.wgsl and tone_map.wgsl and compile their harness."""
+    os.makedirs(out_dir, exist_ok=True)
+    lib = os.path.join(out_dir, "libref_render.so")
+    srcs = [os.path.join(shader_dir, "density.wgsl"), os.path.join(shader_dir, "tone_map.wgsl")]
+    deps = srcs + [os.path.abspath(__file__), os.path.join(HERE, "wgsl_prelude.h"),
+                   os.path.join(HERE, "ref_render_harness.cpp")]
+    if (not force and os.path.exists(lib)
+            and all(os.path.getmtime(d) <= os.path.getmtime(lib) for d in deps)):
+        return lib
+    for path, ns, name in ((srcs[0], "ref_density", "ref_density.inc"),
+                           (srcs[1], "ref_tone_map", "ref_tone_map.inc")):
+        with open(path) as f:
+            text = translate_render(f.read(), ns)
+        with open(os.path.join(out_dir, name), "w") as f:
+            f.write(f"// Generated from {os.path.basename(path)} by oracle/wgsl_to_cpp.py; do not edit.\n")
+            f.write(text)
+    cxx = shutil.which("g++") or "c++"
+    tmp = lib + ".tmp"
+    subprocess.run([cxx, "-O2", "-march=x86-64-v2", "-std=c++17", "-ffp-contract=off",
+                    "-fno-fast-math", "-fPIC", "-shared", "-I", HERE, "-I", out_dir, "-o", tmp,
+                    os.path.join(HERE, "ref_render_harness.cpp")], check=True)
+    os.replace(tmp, lib)
+    return lib
 
 
 def build(shader_dir: str, out_dir: str, force: bool = False) -> str:

@@ -1,5 +1,11 @@
 """Generate the golden fixtures of tests/golden/ from the reference's own shaders.
 
+Render fixture (render_fragments.npz): the translated fragment stages of
+density.wgsl and tone_map.wgsl (oracle/_ref/libref_render.so) evaluated on
+seeded quad coordinates, radius multipliers and camera half sizes (density
+added or discarded), on r16float texel values (tone-mapped rgb) and on
+colormap arguments.
+
 Run in the build container, where the reference checkout exists:
 
     python tests/golden/make_golden.py
@@ -61,6 +67,35 @@ def main() -> None:
                             steps=np.int32(steps), seed=np.int64(seed),
                             pos_n=last["pos"], vel_n=last["vel"], **out)
         print("wrote", case_path(scenario, n))
+    render_fixture(orc)
+
+
+def render_fixture(orc) -> None:
+    if not orc.ref_render_available():
+        raise SystemExit("oracle/_ref/libref_render.so is missing")
+    rng = np.random.default_rng(2024)
+    uv = rng.uniform(-1.05, 1.05, size=(2000, 2)).astype(np.float32)
+    uv = np.concatenate([uv, np.array([[0, 0], [1, 0], [0, -1], [0.6, 0.8], [0.5, 0.5]],
+                                      np.float32)])
+    rms = np.array([0.5, 1.0, 1.0001, 5.0, 12.0], np.float32)
+    halves = np.array([[10.0, 10.0], [16.0, 9.0], [40.0, 20.0], [0.5, 0.25]], np.float32)
+    dens = np.zeros((len(halves), len(rms), len(uv)), np.float32)
+    disc = np.zeros(dens.shape, np.uint8)
+    for a, (hx, hy) in enumerate(halves):
+        for b, rm in enumerate(rms):
+            for c, (ux, uy) in enumerate(uv):
+                dens[a, b, c], disc[a, b, c] = orc.ref_density_fragment(ux, uy, rm, hx, hy)
+    # every 8th finite non-negative FP16 value, and a few fixed ones
+    halfs = np.arange(0, 0x7C00, 8, dtype=np.uint16).view(np.float16).astype(np.float32)
+    texels = np.concatenate([halfs, np.float32([0.125, 1.0, 1e-3, 6e4])])
+    rgb = np.stack([orc.ref_tone_map_fragment(t) for t in texels]).astype(np.float32)
+    ts = np.linspace(-0.1, 1.1, 1201, dtype=np.float32)
+    cmap = np.stack([orc.ref_colormap(t) for t in ts])
+    path = os.path.join(HERE, "render_fragments.npz")
+    np.savez_compressed(path, uv=uv, radius_multipliers=rms, half_sizes=halves, density=dens,
+                        discarded=disc, texels=texels, rgb=rgb, colormap_t=ts,
+                        colormap_rgb=cmap.astype(np.float32))
+    print("wrote", path)
 
 
 if __name__ == "__main__":
