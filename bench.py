@@ -629,7 +629,7 @@ def run_own(args):
         hbm = peaks.get("hbm_gbs", 6650.0)
         kps = sim.kernels_per_step()
         cb = None
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:  # the CPU baseline runs at N = 1 only
             cb = cpu_baseline(pkg, wl)
         out = {
             "metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world,
@@ -668,7 +668,11 @@ def run_own(args):
             "wall_s_timed_region": wall,
         }
     sim.close()
-    if rank == 0:
+    # The secondary points (16.8M, adjoint, ensemble, render, generators) are
+    # single-GPU measurements: a multi-GPU run skips them, so the other ranks
+    # do not wait on rank 0 for minutes at the closing barrier.
+    extras = world == 1
+    if rank == 0 and extras:
         if not args.no_secondary and args.workload != "gaussian-mixture-16m":
             out["secondary"] = secondary_16m(pkg, local)
         if not args.no_adjoint:
@@ -679,6 +683,7 @@ def run_own(args):
             out["render"] = render_cost(pkg, local)
         if not args.no_secondary:
             out["generate"] = generate_cost(pkg, local)
+    if rank == 0:
         print(json.dumps(out))
     if dist is not None:
         dist.barrier()
