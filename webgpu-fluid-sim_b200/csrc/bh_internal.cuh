@@ -132,6 +132,7 @@ struct DeviceBuffers {
     float2* vel = nullptr;
     float2* acc = nullptr;
     float* radius = nullptr;
+    float4* xm = nullptr;   // {x, y, m, 0} per body (original order), written by the encode
     // sort
     void* codes = nullptr;      // sorted keys after a step
     void* codes_alt = nullptr;

@@ -261,7 +261,7 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     const uint32_t tiles = (uint32_t)((n + bh::kSortTile - 1) / bh::kSortTile);
     Carver c;
     size_t o_mass = c.take<float>(nb), o_pos = c.take<float2>(nb), o_vel = c.take<float2>(nb);
-    size_t o_acc = c.take<float2>(nb), o_rad = c.take<float>(nb);
+    size_t o_acc = c.take<float2>(nb), o_rad = c.take<float>(nb), o_xm = c.take<float4>(nb);
     size_t o_codes = c.take<uint8_t>(nb * kb), o_codes2 = c.take<uint8_t>(nb * kb);
     size_t o_ids = c.take<uint32_t>(nb), o_ids2 = c.take<uint32_t>(nb);
     size_t o_node4 = c.take<float4>(nn), o_child = c.take<uint2>(ni), o_parent = c.take<uint32_t>(nn);
@@ -294,6 +294,7 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     b.vel = (float2*)(a + o_vel);
     b.acc = (float2*)(a + o_acc);
     b.radius = (float*)(a + o_rad);
+    b.xm = (float4*)(a + o_xm);
     b.codes = a + o_codes;
     b.codes_alt = a + o_codes2;
     b.ids = (uint32_t*)(a + o_ids);

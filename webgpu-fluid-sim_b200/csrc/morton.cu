@@ -158,7 +158,9 @@ __device__ __forceinline__ uint64_t encode_one<uint64_t>(float x, float y, const
 template <typename K>
 __global__ void __launch_bounds__(256) encode_kernel(const float4* __restrict__ pos2, uint32_t n,
                                                      K* __restrict__ codes, int domain,
-                                                     StepScratch* scratch) {
+                                                     StepScratch* scratch,
+                                                     const float* __restrict__ mass,
+                                                     float4* __restrict__ xm) {
     constexpr int P = (int)sizeof(K);  // digit passes = key bytes
     __shared__ uint32_t sh[P][kRadix];
     for (int i = threadIdx.x; i < P * kRadix; i += blockDim.x) (&sh[0][0])[i] = 0;
@@ -175,6 +177,12 @@ __global__ void __launch_bounds__(256) encode_kernel(const float4* __restrict__ 
         }
         K k0 = encode_one<K>(v.x, v.y, d);
         codes[b0] = k0;
+        // the body records the hierarchy build gathers by sorted id: one
+        // 16-B load there instead of a position and a mass
+        if (xm) {
+            xm[b0] = make_float4(v.x, v.y, __ldg(&mass[b0]), 0.0f);
+            if (b0 + 1 < n) xm[b0 + 1] = make_float4(v.z, v.w, __ldg(&mass[b0 + 1]), 0.0f);
+        }
 #pragma unroll
         for (int p = 0; p < P; ++p) atomicAdd(&sh[p][(uint32_t)(k0 >> (8 * p)) & 0xFFu], 1u);
         if (b0 + 1 < n) {
@@ -199,9 +207,11 @@ void launch_encode(const DeviceBuffers& b, int domain, cudaStream_t s) {
     if (blocks < 1) blocks = 1;
     const float4* p2 = reinterpret_cast<const float4*>(b.pos);
     if (b.key_bytes == 8)
-        encode_kernel<uint64_t><<<blocks, 256, 0, s>>>(p2, b.n, (uint64_t*)b.codes, domain, b.scratch);
+        encode_kernel<uint64_t><<<blocks, 256, 0, s>>>(p2, b.n, (uint64_t*)b.codes, domain, b.scratch,
+                                                       b.mass, b.xm);
     else
-        encode_kernel<uint32_t><<<blocks, 256, 0, s>>>(p2, b.n, (uint32_t*)b.codes, domain, b.scratch);
+        encode_kernel<uint32_t><<<blocks, 256, 0, s>>>(p2, b.n, (uint32_t*)b.codes, domain, b.scratch,
+                                                       b.mass, b.xm);
 }
 
 // ---- ensembles: one box and one 32-bit Morton domain per system ----------
@@ -248,7 +258,9 @@ __global__ void __launch_bounds__(256) encode_ensemble_kernel(const float2* __re
                                                               const uint32_t* __restrict__ sys_bbox,
                                                               uint32_t n, int passes,
                                                               uint64_t* __restrict__ codes,
-                                                              StepScratch* scratch) {
+                                                              StepScratch* scratch,
+                                                              const float* __restrict__ mass,
+                                                              float4* __restrict__ xm) {
     __shared__ uint32_t sh[8][kRadix];
     for (int i = threadIdx.x; i < 8 * kRadix; i += blockDim.x) (&sh[0][0])[i] = 0;
     __syncthreads();
@@ -267,6 +279,7 @@ __global__ void __launch_bounds__(256) encode_ensemble_kernel(const float2* __re
             const uint32_t m = spread16(quant16(p.x, mnx, ext)) | (spread16(quant16(p.y, mny, ext)) << 1);
             k = ((uint64_t)sys << 32) | m;
             codes[i] = k;
+            if (xm) xm[i] = make_float4(p.x, p.y, __ldg(&mass[i]), 0.0f);
         }
         // Morton digits are spread out: one shared atomic per body.  System
         // digits repeat across a warp: one atomic per distinct digit.
@@ -293,7 +306,7 @@ void launch_encode_ensemble(const DeviceBuffers& b, cudaStream_t s) {
     int blocks = (int)((b.n + 255) / 256);
     if (blocks > 148 * 4) blocks = 148 * 4;
     encode_ensemble_kernel<<<blocks, 256, 0, s>>>(b.pos, b.body_sys, b.sys_bbox, b.n, b.sort_passes,
-                                                  (uint64_t*)b.codes, b.scratch);
+                                                  (uint64_t*)b.codes, b.scratch, b.mass, b.xm);
 }
 
 // ---- leapfrog opening kick + drift (original order, coalesced) -----------

@@ -32,6 +32,7 @@ static void launch_typed(const DeviceBuffers& b, int fp64_levels, cudaStream_t s
     a.groups = b.groups;
     a.group_count = b.groups ? &b.scratch->group_ctr[1] : nullptr;
     a.gmax = b.group_max;
+    a.xm = b.xm;
     const uint32_t grid = (b.n + kBuildBlock - 1) / kBuildBlock;
     if (!split_build(b.n)) {
         build_fill_kernel<K, false><<<grid, kBuildBlock, 0, s>>>(a);

@@ -93,6 +93,9 @@ struct BuildArgs {
     // slot, last slot}, and their count (zero before the local phase).
     uint2* frontier = nullptr;
     unsigned int* frontier_count = nullptr;
+    // {x, y, m, 0} per body in original order, when the encode wrote them:
+    // one gather per slot instead of a position and a mass
+    const float4* xm = nullptr;
 };
 
 // One thread per sorted slot climbs from its leaf; the lanes of a warp start
@@ -425,8 +428,16 @@ build_fill_kernel(const BuildArgs<K> A) {
     if (i >= n) return;
 
     const uint32_t body = __ldg(&A.ids[i]);
-    const float m = __ldg(&A.mass[body]);
-    const float2 p = __ldg(&A.pos[body]);
+    float m;
+    float2 p;
+    if (A.xm) {
+        const float4 r = __ldg(&A.xm[body]);
+        m = r.z;
+        p = make_float2(r.x, r.y);
+    } else {
+        m = __ldg(&A.mass[body]);
+        p = __ldg(&A.pos[body]);
+    }
     A.node4[nm1 + i] = make_float4(p.x, p.y, m, 0.0f);  // leaf (lbvh.wgsl:179-187)
     S.leaf[0][t] = m;
     S.leaf[1][t] = p.x;
