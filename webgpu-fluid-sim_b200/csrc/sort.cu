@@ -10,13 +10,14 @@
 //  - The digit histograms of every pass come from the encode kernel, so each
 //    pass reads its keys exactly once.
 //  - A CTA takes the next tile (kSortTile keys) from an atomic counter (so lower
-//    tiles are always already running), ranks its keys warp by warp with
-//    __match_any_sync (stable: item-major, lane-minor = memory order),
-//    publishes its per-digit counts, and resolves its global offsets by a
-//    decoupled look-back over the tiles before it.  The look-back spin is
-//    bounded; on giving up it raises kErrLookbackSpin instead of hanging.
-//  - Keys and ids are staged in shared memory in digit order and written out
-//    in runs, so global stores are contiguous per digit.
+//    tiles are always already running), ranks its keys warp by warp with a
+//    ballot multisplit (stable: item-major, lane-minor = memory order),
+//    publishes its per-digit counts, stages the tile in shared memory in
+//    digit order, and then resolves its global offsets by a decoupled
+//    look-back over the tiles before it, several tiles per round trip.  The look-back spin is bounded; on giving up it raises
+//    kErrLookbackSpin instead of hanging.
+//  - Staged keys and ids are written out in runs, so global stores are
+//    contiguous per digit.
 //  - Pass 0 does not read ids: it writes the identity permutation of
 //    lbvh.wgsl:68 directly.
 //  - With an even number of passes (4 for 32-bit keys, 8 for 64-bit keys)
@@ -32,6 +33,10 @@ constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kFlagMask = 3u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1;
 constexpr uint32_t kSpinCap = 1u << 22;
+#ifndef BH_SORT_LOOK_BATCH
+#define BH_SORT_LOOK_BATCH 4
+#endif
+constexpr int kLookBatch = BH_SORT_LOOK_BATCH;  // predecessor tiles read per look-back round
 
 // Exclusive scan over the block (every thread takes part; threads past the
 // 256 digits pass 0, so the digits' prefixes are unaffected by them).
@@ -95,14 +100,24 @@ onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_
             id[k] = 0;
         }
     }
-    // Warp-local stable ranking.
+    // Warp-local stable ranking.  The lanes holding the same digit are found
+    // by eight ballots, one per digit bit (warp multisplit): a constant cost,
+    // where a match instruction slows down with the number of distinct
+    // digits in the warp.
+    const bool full_tile = tile * (uint32_t)kSortTile + (uint32_t)kSortTile <= n;
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         uint32_t idx = seg + (uint32_t)k * 32u + (uint32_t)lane;
         bool valid = idx < n;
         uint32_t d = (uint32_t)(key[k] >> shift) & 0xFFu;
-        uint32_t tag = valid ? d : 256u + (uint32_t)lane;
-        unsigned peers = __match_any_sync(0xFFFFFFFFu, tag);
+        unsigned peers = full_tile ? 0xFFFFFFFFu : __ballot_sync(0xFFFFFFFFu, valid);
+#pragma unroll
+        for (int bit = 0; bit < kRadixBits; ++bit) {
+            const bool on = (d >> bit) & 1u;
+            const unsigned vote = __ballot_sync(0xFFFFFFFFu, on);
+            peers &= on ? vote : ~vote;
+        }
+        if (!valid) peers = 1u << lane;
         int leader = __ffs(peers) - 1;
         uint32_t below = __popc(peers & ((1u << lane) - 1u));
         uint32_t base = 0;
@@ -137,36 +152,10 @@ onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_
     }
     const uint32_t tile_excl = block_excl_scan(tile_cnt, s_tot);
     const uint32_t glob_excl = block_excl_scan(digit_thread ? scratch->hist[pass][d] : 0u, s_tot);
-    // Decoupled look-back over earlier tiles, one digit per thread.
-    uint32_t excl = 0;
-    if (tile > 0 && digit_thread) {
-        int t = (int)tile - 1;
-        uint32_t spins = 0;
-        while (true) {
-            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> a(
-                status[((size_t)pass * tiles + (uint32_t)t) * kRadix + d]);
-            uint32_t v = a.load(cuda::memory_order_relaxed);
-            if ((v & kFlagMask) == 0u) {
-                if (++spins > kSpinCap) {
-                    atomicOr(err, kErrLookbackSpin);
-                    break;
-                }
-                if (spins > 64) __nanosleep(64);
-                continue;
-            }
-            excl += v & kValueMask;
-            if ((v & kFlagMask) == kFlagPrefix || t == 0) break;
-            --t;
-        }
-        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> a(my_status[d]);
-        a.store(kFlagPrefix | (excl + tile_cnt), cuda::memory_order_relaxed);
-    }
-    if (digit_thread) {
-        s_tile_excl[d] = tile_excl;
-        s_gbase[d] = glob_excl + excl;
-    }
+    if (digit_thread) s_tile_excl[d] = tile_excl;
     __syncthreads();
-    // Stage in digit order.
+    // Stage in digit order before the look-back: the tile's own work is done
+    // while the tiles before it finish theirs, so the walk back is shorter.
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         uint32_t idx = seg + (uint32_t)k * 32u + (uint32_t)lane;
@@ -177,6 +166,48 @@ onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_
             s_ids[p] = id[k];
         }
     }
+    // Decoupled look-back over earlier tiles, one digit per thread, reading
+    // kLookBatch tiles per round trip (nearest first): the values are used up
+    // to the first inclusive prefix, and re-read from the first tile that has
+    // not published yet.
+    uint32_t excl = 0;
+    if (tile > 0 && digit_thread) {
+        uint32_t* st = status + (size_t)pass * tiles * kRadix + d;
+        int t = (int)tile - 1;
+        uint32_t spins = 0;
+        while (true) {
+            uint32_t v[kLookBatch];
+#pragma unroll
+            for (int j = 0; j < kLookBatch; ++j) {
+                v[j] = kFlagPrefix;  // below tile 0: never used
+                if (t - j >= 0) {
+                    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> a(st[(size_t)(t - j) * kRadix]);
+                    v[j] = a.load(cuda::memory_order_relaxed);
+                }
+            }
+            bool done = false;
+            int used = 0;
+#pragma unroll
+            for (int j = 0; j < kLookBatch; ++j) {
+                if (done || used < j || (v[j] & kFlagMask) == 0u) continue;
+                excl += v[j] & kValueMask;
+                used = j + 1;
+                done = (v[j] & kFlagMask) == kFlagPrefix || t - j == 0;
+            }
+            if (done) break;
+            t -= used;
+            if (used == 0) {
+                if (++spins > kSpinCap) {
+                    atomicOr(err, kErrLookbackSpin);
+                    break;
+                }
+                if (spins > 64) __nanosleep(64);
+            }
+        }
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> a(my_status[d]);
+        a.store(kFlagPrefix | (excl + tile_cnt), cuda::memory_order_relaxed);
+    }
+    if (digit_thread) s_gbase[d] = glob_excl + excl;
     __syncthreads();
     const uint32_t tile_base = tile * kSortTile;
     const uint32_t tile_n = (n - tile_base) < (uint32_t)kSortTile ? (n - tile_base) : (uint32_t)kSortTile;
