@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--walk-shape", default=None, metavar="BPL,LEAF",
+                    help="pin the group walk's bodies_per_lane and leaf size (no autotuner): "
+                         "profiling runs use the shape a plain run picked")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
@@ -468,6 +471,12 @@ def run_reference(args):
 
 # ---------------------------------------------------------------- own arm
 
+def _rel_change(new: float, old: float):
+    """(new - old) / |old|, or None when the starting value is exactly zero
+    (a system at rest in angular momentum, e.g. the Gaussian mixture)."""
+    return (new - old) / abs(old) if old != 0.0 else None
+
+
 def run_own(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -484,6 +493,10 @@ def run_own(args):
     wl = pkg.WORKLOADS[args.workload]
     cfg = wl["config"]
     n = wl["n"]
+    if args.walk_shape:
+        bpl, leaf = (int(v) for v in args.walk_shape.split(","))
+        cfg = dataclasses.replace(cfg, bodiesPerLane=bpl, leafSize=leaf)
+        args.no_autotune = True
     sharded = None
     if args.shard:
         # One system on all ranks: rank 0 picks the walk shape, everyone uses it
@@ -642,7 +655,7 @@ def run_own(args):
                        "integrator": cfg.integrator, "morton_bits": cfg.mortonBits,
                        "walk": f"{cfg.walk}, multipole order {cfg.multipole}",
                        "bodies_per_lane": cfg.bodiesPerLane, "leaf_size": cfg.leafSize,
-                       "autotuned": tune is not None,
+                       "autotuned": tune is not None, "shape_pinned": bool(args.walk_shape),
                        "parallelism": (f"shard{world} (sorted-slot ranges, one all-gather of "
                                        f"16 B/body per step)" if sharded is not None else
                                        f"replicas{world}" if world > 1 else "single"),
@@ -656,11 +669,11 @@ def run_own(args):
                     "d2h_bytes_per_step": 16 * n, "steps": E},
             "diagnostics": {
                 "steps": args.warmup + K,
-                "energy_drift": (diag1["total_energy"] - diag0["total_energy"])
-                                / abs(diag0["total_energy"]),
+                "energy_drift": _rel_change(diag1["total_energy"], diag0["total_energy"]),
                 "momentum_change": [a - b for a, b in zip(diag1["momentum"], diag0["momentum"])],
-                "angular_momentum_drift": (diag1["angular_momentum"] - diag0["angular_momentum"])
-                                          / abs(diag0["angular_momentum"]),
+                "angular_momentum_change": diag1["angular_momentum"] - diag0["angular_momentum"],
+                "angular_momentum_drift": _rel_change(diag1["angular_momentum"],
+                                                      diag0["angular_momentum"]),
                 "total_energy_start": diag0["total_energy"],
                 "how": "FP64 sums, direct-sum potential, before warm-up and after the timed steps"},
             "gpu_launches": kps * K,
