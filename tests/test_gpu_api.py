@@ -95,3 +95,59 @@ def test_zero_bodies_step_and_download(bh):
     assert m.shape == (0,) and p.shape == (0, 2)
     assert s.computeAccelerations().shape == (0, 2)
     s.close()
+
+
+def _pinned(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).pin_memory()
+
+
+@pytest.mark.parametrize("integrator,walk", [("symplectic-euler", "group"),
+                                             ("symplectic-euler", "exact"),
+                                             ("leapfrog-kdk", "group")])
+def test_velocity_upload_overlapping_the_tree_stages(bh, integrator, walk):
+    """Uploaded velocities cross PCIe on a copy stream while the next step's
+    tree stages run; the results must be those of waiting for the upload."""
+    cfg = dict(integrator=integrator, walk=walk, softening="plummer", plummerEps=1e-3,
+               mortonDomain="bbox", deltaTime=1e-3)
+    a = _sim(bh, n=20000, **cfg)
+    b = _sim(bh, n=20000, **cfg)
+    m, p, v = a.download()
+    keep = []  # page-locked host arrays stay alive until the copies are done
+    for k in range(3):
+        hm, hp, hv = _pinned(m), _pinned(p * (1.0 + 0.01 * k)), _pinned(v * (1.0 + 0.5 * k))
+        keep.append((hm, hp, hv))
+        a.upload(hm, hp, hv)
+        a.step(2)            # no wait between the upload and the step
+        b.upload(hm, hp, hv)
+        b.sync()             # the upload has landed before the step
+        b.step(2)
+    for x, y in zip(a.download(), b.download()):
+        assert np.array_equal(x, y)
+    a.close()
+    b.close()
+
+
+def test_velocity_upload_then_other_calls(bh):
+    """Every call after an upload sees its velocities: a download, the
+    diagnostics, a borrowed-buffer read, and a body-count change."""
+    s = _sim(bh, n=4000)
+    rng = np.random.default_rng(5)
+    v = rng.standard_normal((4000, 2)).astype(np.float32)
+    hv = _pinned(v)
+    s.upload(None, None, hv)
+    assert np.array_equal(s.download()[2], v)
+    hv2 = _pinned(2 * v)
+    s.upload(None, None, hv2)
+    assert np.array_equal(s.read_buffer("vel", np.float32, 8000).reshape(-1, 2), 2 * v)
+    m = s.download()[0].astype(np.float64)
+    s.upload(None, None, hv)
+    d = s.diagnostics(potential=False)
+    ke = 0.5 * float(np.sum(m * np.sum(v.astype(np.float64) ** 2, axis=1)))
+    assert d["kinetic_energy"] == pytest.approx(ke, rel=1e-9)
+    s.upload(None, None, hv2)
+    s.setNumBodies(3000)       # reallocates while the copy may be in flight
+    s.step(1)
+    s.sync()
+    assert s.download()[2].shape == (3000, 2)
+    s.close()

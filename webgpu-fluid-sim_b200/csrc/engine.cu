@@ -39,9 +39,17 @@ struct bh_sim {
     void* arena = nullptr;
     size_t arena_bytes = 0;
     bool acc_valid = false;
-    // graphs: [0] plain, [1] with event-record nodes at the stage boundaries
-    cudaGraph_t graph[2] = {nullptr, nullptr};
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    // graphs: [0] plain, [1] with event-record nodes at the stage boundaries,
+    // [2] the tree stages alone and [3] the walk alone (the first step after an
+    // upload whose velocities are still being copied, see bh_upload)
+    cudaGraph_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};
+    // Uploaded velocities cross PCIe on copy_stream, ordered after the
+    // stream's earlier work (ev_copy_order); the stream waits on ev_vel before
+    // the next use of the velocities (settle_vel).
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_copy_order = nullptr, ev_vel = nullptr;
+    mutable bool vel_pending = false;
     cudaGraphNode_t ev_node[kMarkers] = {};
     cudaEvent_t markers[kMarkers] = {};
     // profiling
@@ -72,6 +80,16 @@ struct bh_sim {
 
 static thread_local std::string g_err;
 
+// Orders the handle's stream after a velocity upload still in flight on the
+// copy stream.  Every entry point calls it (through BH_HANDLE) before it
+// touches the body buffers, except bh_upload and bh_step, which order the
+// copy themselves.
+static void settle_vel(const bh_sim* s) {
+    if (!s->vel_pending) return;
+    cudaStreamWaitEvent(s->stream, s->ev_vel, 0);
+    s->vel_pending = false;
+}
+
 namespace bh {
 // Message for bh_global_last_error() from entry points without a handle.
 void set_global_error(const std::string& msg) { g_err = msg; }
@@ -82,6 +100,7 @@ namespace bh {
 // refreshes the reference node layout); false for a null handle.
 bool sim_body_view(const bh_sim* s, BodyView* out) {
     if (!s || !out) return false;
+    settle_vel(s);  // callers use the buffers on the handle's stream
     out->mass = s->b.mass;
     out->pos = s->b.pos;
     out->vel = s->b.vel;
@@ -167,7 +186,7 @@ static int validate_config(bh_sim* s, const bh_config& c) {
 // ---- buffers --------------------------------------------------------------
 
 static void destroy_graphs(bh_sim* s) {
-    for (int v = 0; v < 2; ++v) {
+    for (int v = 0; v < 4; ++v) {
         if (s->exec[v]) cudaGraphExecDestroy(s->exec[v]);
         if (s->graph[v]) cudaGraphDestroy(s->graph[v]);
         s->exec[v] = nullptr;
@@ -234,6 +253,8 @@ static int save_tree(bh_sim* s, uint32_t k) {
 }
 
 static void free_buffers(bh_sim* s) {
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);  // no copy into freed memory
+    s->vel_pending = false;
     destroy_graphs(s);
     free_adjoint(s);
     if (s->arena) cudaFree(s->arena);
@@ -435,9 +456,15 @@ static void enqueue_forces(bh_sim* s, Mark mark) {
 static int capture_graph(bh_sim* s, int variant) {
     cudaStream_t st = s->stream;
     BH_CUDA(s, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(s, [&](int k) {
-        if (variant == 1) cudaEventRecordWithFlags(s->markers[k], st, cudaEventRecordExternal);
-    });
+    if (variant == 2) {
+        enqueue_tree(s, [](int) {});  // symplectic Euler: the step's stages before the walk
+    } else if (variant == 3) {
+        launch_walk_any(s, walk_params(s, bh::kWalkEulerKickDrift));
+    } else {
+        enqueue_step(s, [&](int k) {
+            if (variant == 1) cudaEventRecordWithFlags(s->markers[k], st, cudaEventRecordExternal);
+        });
+    }
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (e != cudaSuccess) return cuda_fail(s, e, "cudaStreamEndCapture(step)");
@@ -500,11 +527,16 @@ static int check_device_errors(bh_sim* s) {
     return fail(s, BH_ERR_DEVICE_CHECK, msg);
 }
 
-#define BH_HANDLE(s)                                                                        \
+#define BH_HANDLE_NO_SETTLE(s)                                                              \
     do {                                                                                    \
         if (!(s)) return fail(nullptr, BH_ERR_INVALID_ARGUMENT, "null bh_sim handle");      \
         cudaError_t _d = cudaSetDevice((s)->device);                                        \
         if (_d != cudaSuccess) return cuda_fail((s), _d, "cudaSetDevice");                  \
+    } while (0)
+#define BH_HANDLE(s)                                                                        \
+    do {                                                                                    \
+        BH_HANDLE_NO_SETTLE(s);                                                             \
+        settle_vel(s);                                                                      \
     } while (0)
 
 // ---- lifetime ------------------------------------------------------------------
@@ -579,6 +611,9 @@ static int create_sim(const bh_config* config, const uint32_t* sizes, uint32_t n
     s->device = s->cfg.device;
     if ((e = cudaSetDevice(s->device)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&s->ev_copy_order, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&s->ev_vel, cudaEventDisableTiming)) != cudaSuccess ||
         (e = bh::sort_init_attributes()) != cudaSuccess) {
         int r = cuda_fail(nullptr, e, "bh_create");
         delete s;
@@ -617,6 +652,9 @@ extern "C" int bh_destroy(bh_sim* s) {
     free_profile(s);
     for (int k = 0; k < kMarkers; ++k)
         if (s->markers[k]) cudaEventDestroy(s->markers[k]);
+    if (s->ev_vel) cudaEventDestroy(s->ev_vel);
+    if (s->ev_copy_order) cudaEventDestroy(s->ev_copy_order);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return BH_OK;
@@ -772,12 +810,22 @@ extern "C" int bh_update_metadata(bh_sim* s) {
 }
 
 extern "C" int bh_upload(bh_sim* s, const float* mass, const float* pos, const float* vel, uint32_t n) {
-    BH_HANDLE(s);
+    BH_HANDLE_NO_SETTLE(s);
     if (n != s->b.n) return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_upload: n differs from the body count");
     if (n == 0) return BH_OK;
     if (mass) BH_CUDA(s, cudaMemcpyAsync(s->b.mass, mass, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
     if (pos) BH_CUDA(s, cudaMemcpyAsync(s->b.pos, pos, 8 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
-    if (vel) BH_CUDA(s, cudaMemcpyAsync(s->b.vel, vel, 8 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    if (vel) {
+        // On the copy stream, after everything enqueued so far on the handle's
+        // stream (so after the mass and position copies, and after any step
+        // still reading or writing the velocities); the next step's tree
+        // stages do not wait for it (step_once), every other call does.
+        BH_CUDA(s, cudaEventRecord(s->ev_copy_order, s->stream));
+        BH_CUDA(s, cudaStreamWaitEvent(s->copy_stream, s->ev_copy_order, 0));
+        BH_CUDA(s, cudaMemcpyAsync(s->b.vel, vel, 8 * (size_t)n, cudaMemcpyHostToDevice, s->copy_stream));
+        BH_CUDA(s, cudaEventRecord(s->ev_vel, s->copy_stream));
+        s->vel_pending = true;
+    }
     if (mass || pos) s->acc_valid = false;
     return BH_OK;
 }
@@ -803,6 +851,22 @@ static int step_once(bh_sim* s) {
         s->acc_valid = true;
     }
     cudaEvent_t* ev = prof_slot(s);
+    if (s->vel_pending && !kdk && !ev && s->cfg.use_graphs) {
+        // The last upload's velocities are still crossing PCIe on the copy
+        // stream; the walk is their first reader, so the tree stages run
+        // meanwhile (the same kernels in the same order as the whole-step graph).
+        for (int v = 2; v < 4; ++v)
+            if (!s->exec[v]) {
+                int rc = capture_graph(s, v);
+                if (rc != BH_OK) return rc;
+            }
+        BH_CUDA(s, cudaGraphLaunch(s->exec[2], s->stream));
+        settle_vel(s);
+        BH_CUDA(s, cudaGraphLaunch(s->exec[3], s->stream));
+        s->acc_valid = false;
+        return BH_OK;
+    }
+    settle_vel(s);
     if (s->cfg.use_graphs) {
         const int v = ev ? 1 : 0;
         if (!s->exec[v]) {
@@ -825,7 +889,7 @@ static int step_once(bh_sim* s) {
 }
 
 extern "C" int bh_step(bh_sim* s, uint32_t frames) {
-    BH_HANDLE(s);
+    BH_HANDLE_NO_SETTLE(s);  // step_once orders a pending velocity upload
     if (s->b.n == 0) return BH_OK;
     const uint64_t steps = (uint64_t)frames * (uint64_t)s->cfg.substeps;  // simulation.ts:393
     for (uint64_t i = 0; i < steps; ++i) {
