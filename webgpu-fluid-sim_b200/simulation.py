@@ -154,6 +154,7 @@ class Simulation:
 
     def sync(self) -> None:
         self._check(self._lib.bh_sync(self._h))
+        self._pending_host = []
 
     def upload(self, mass=None, pos=None, vel=None) -> None:
         n = self.getNumBodies()
@@ -164,7 +165,9 @@ class Simulation:
                 continue
             a = _as_host_f32(a, n * width)
             args.append(a)
-        self._keep = args  # host memory must outlive the asynchronous copy
+        # Host memory must outlive the asynchronous copies: held until the next
+        # sync or download, which wait for them.
+        self._pending_host = getattr(self, "_pending_host", []) + [args]
         ptrs = [_ptr(a) for a in args]
         self._check(self._lib.bh_upload(self._h, *ptrs, n))
 
@@ -174,12 +177,14 @@ class Simulation:
         pos = np.empty((n, 2), np.float32)
         vel = np.empty((n, 2), np.float32)
         self._check(self._lib.bh_download(self._h, _ptr(mass), _ptr(pos), _ptr(vel), n))
+        self._pending_host = []
         return mass, pos, vel
 
     def download_into(self, mass=None, pos=None, vel=None) -> None:
         """Download into caller-owned host arrays (page-locked for async speed)."""
         n = self.getNumBodies()
         self._check(self._lib.bh_download(self._h, _ptr(mass), _ptr(pos), _ptr(vel), n))
+        self._pending_host = []
 
     def computeAccelerations(self) -> np.ndarray:
         n = self.getNumBodies()
