@@ -33,14 +33,16 @@ static void launch_typed(const DeviceBuffers& b, int fp64_levels, cudaStream_t s
     a.group_count = b.groups ? &b.scratch->group_ctr[1] : nullptr;
     a.gmax = b.group_max;
     a.xm = b.xm;
-    const uint32_t grid = (b.n + kBuildBlock - 1) / kBuildBlock;
     if (!split_build(b.n)) {
-        build_fill_kernel<K, false><<<grid, kBuildBlock, 0, s>>>(a);
+        constexpr uint32_t B = build_block<false>();
+        build_fill_kernel<K, false><<<(b.n + B - 1) / B, B, 0, s>>>(a);
         return;
     }
     a.frontier = b.frontier;
     a.frontier_count = &b.scratch->frontier_ctr;
-    build_fill_kernel<K, true><<<grid, kBuildBlock, 0, s>>>(a);
+    constexpr uint32_t B = build_block<true>();
+    const uint32_t grid = (b.n + B - 1) / B;
+    build_fill_kernel<K, true><<<grid, B, 0, s>>>(a);
     // Frontier nodes number far fewer than bodies (a handful per CTA), but
     // only the device knows how many: a resident grid strides over them.
     static int blocks_per_sm[64] = {};
@@ -48,14 +50,14 @@ static void launch_typed(const DeviceBuffers& b, int fp64_levels, cudaStream_t s
     cudaGetDevice(&dev);
     int& bps = blocks_per_sm[dev & 63];
     if (bps == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, build_climb_kernel<K>, kBuildBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, build_climb_kernel<K>, kClimbBlock, 0);
         if (bps < 1) bps = 1;
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     uint32_t blocks = (uint32_t)(sms * bps);
     if (blocks > grid) blocks = grid;
-    build_climb_kernel<K><<<blocks, kBuildBlock, 0, s>>>(a);
+    build_climb_kernel<K><<<blocks, kClimbBlock, 0, s>>>(a);
 }
 
 // Reference-layout internal-node arrays from the packed records: node4

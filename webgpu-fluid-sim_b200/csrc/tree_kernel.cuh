@@ -26,7 +26,8 @@
 // through L2 (__ldcg), so no stale data is ever combined.  There are no spins.
 // bound[] holds kSentinel between steps: the second arriver restores it.
 //
-// Two phases per climb.  A CTA owns 256 consecutive slots.  A node whose
+// Two phases per climb.  A CTA owns B consecutive slots (128 in the fused
+// build, 512 in the split build's local phase).  A node whose
 // range lies inside those slots ("local") is combined through shared memory:
 // its split's exchange slot is a shared-memory word, the sibling's record is
 // read from shared memory, and block-scope fences suffice.  Which splits are
@@ -38,8 +39,8 @@
 // are among the CTA's own, i.e. when the prefix and suffix minima of the
 // CTA's deltas around g are below delta(g).  A climb leaves the local phase
 // at the first split that is not local and continues with the device-scope
-// protocol above.  Local nodes hold < 256 bodies, so they all take the f32
-// path below.
+// protocol above.  Local nodes hold < B < 1024 bodies, so they all take the
+// f32 path below.
 //
 // Mass / COM: small nodes use the reference's f32 formula
 //   M = m_l + m_r;  com = (c_l m_l + c_r m_r) / M  (0 if M <= 0)   (lbvh.wgsl:216-224)
@@ -102,20 +103,29 @@ struct BuildArgs {
 // at adjacent leaves, so the low levels they create are adjacent in memory.
 // (A persistent variant that hands each finished lane a new leaf measured
 // slower at 16M bodies: its lanes drift apart and its node writes scatter.)
-constexpr int kBuildBlock = 256;
-static_assert(kFp64MinBodies > kBuildBlock, "local nodes must all take the f32 path");
+// Slots per CTA (measured, B200): the fused build is fastest with small CTAs
+// (800k bodies: 128 -> 0.137 ms, 256 -> 0.140, 512 -> 0.150), the local phase
+// of the split build with large ones (16.8M: 128 -> 2.11 ms, 256 -> 1.83,
+// 512 -> 1.72).  The frontier climb keeps 256 threads per CTA.
+constexpr int kBuildBlockFused = 128;
+constexpr int kBuildBlockSplit = 512;
+constexpr int kClimbBlock = 256;
+template <bool SPLIT>
+constexpr int build_block() { return SPLIT ? kBuildBlockSplit : kBuildBlockFused; }
+static_assert(kFp64MinBodies > kBuildBlockFused && kFp64MinBodies > kBuildBlockSplit,
+              "local nodes must all take the f32 path");
 
-// The block-local shared state of the local phase.
-template <typename K>
+// The block-local shared state of the local phase (B slots per CTA).
+template <typename K, int B>
 struct BuildShared {
-    K key[kBuildBlock + 2];           // keys of slots B0-1 .. B0+B
-    int d[kBuildBlock + 1];           // delta at boundary g = B0-1+q (between slots g, g+1)
-    int wmin[2][kBuildBlock / 32];    // per-warp minima for the two scans
-    int suf[kBuildBlock];             // suf[q] = min of d[q+1..B]
-    unsigned char local[kBuildBlock + 1];
-    uint32_t bound[kBuildBlock + 1];  // exchange slots of the local splits
-    float leaf[3][kBuildBlock];       // leaf {m, x, y} by slot - B0
-    float rec[10][kBuildBlock];       // local internal node {m, cx, cy, box, S} by index - B0
+    K key[B + 2];           // keys of slots B0-1 .. B0+B
+    int d[B + 1];           // delta at boundary g = B0-1+q (between slots g, g+1)
+    int wmin[2][B / 32];    // per-warp minima for the two scans
+    int suf[B];             // suf[q] = min of d[q+1..B]
+    unsigned char local[B + 1];
+    uint32_t bound[B + 1];  // exchange slots of the local splits
+    float leaf[3][B];       // leaf {m, x, y} by slot - B0
+    float rec[10][B];       // local internal node {m, cx, cy, box, S} by index - B0
 };
 
 // The node a climbing thread currently owns: its slot range, the deltas at
@@ -134,14 +144,13 @@ struct Climb {
 // is the first to arrive at the split (it stops; the sibling's thread goes
 // on) or has created the root, else true with `c` holding the parent.
 //   LOCAL: the thread starts in the block-local phase (shared memory `S` of
-//          the CTA owning slots [B0, B0 + kBuildBlock)).
+//          the CTA owning slots [B0, B0 + B)).
 //   STOP:  at the first split that is not local, record the node in the
 //          frontier list and stop (the split build's first kernel); else go
 //          on with the device-scope protocol (fused build, second kernel).
-template <typename K, bool LOCAL, bool STOP>
-__device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, BuildShared<K>* S,
+template <typename K, int B, bool LOCAL, bool STOP>
+__device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, BuildShared<K, B>* S,
                                            uint32_t B0) {
-    constexpr int B = kBuildBlock;
     const uint32_t n = A.n, nm1 = n - 1;
     bool local = LOCAL && c.local;
     volatile float* vrec = LOCAL ? &S->rec[0][0] : nullptr;
@@ -161,7 +170,7 @@ __device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, Buil
             return false;
         }
         // Past the stop test a split build's first kernel is always local;
-        // its nodes hold fewer than kBuildBlock bodies, so never take FP64.
+        // its nodes hold fewer than B bodies, so never take FP64.
         const bool IN_LOCAL = LOCAL && (STOP || local);
         uint32_t other;
         if (IN_LOCAL) {
@@ -338,10 +347,10 @@ __device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, Buil
 }
 
 // The whole climb of one thread.
-template <typename K, bool LOCAL, bool STOP>
-__device__ __forceinline__ void climb(const BuildArgs<K>& A, Climb& c, BuildShared<K>* S,
+template <typename K, int B, bool LOCAL, bool STOP>
+__device__ __forceinline__ void climb(const BuildArgs<K>& A, Climb& c, BuildShared<K, B>* S,
                                       uint32_t B0) {
-    while (climb_step<K, LOCAL, STOP>(A, c, S, B0)) {
+    while (climb_step<K, B, LOCAL, STOP>(A, c, S, B0)) {
     }
 }
 
@@ -358,10 +367,10 @@ __device__ __forceinline__ void climb(const BuildArgs<K>& A, Climb& c, BuildShar
 // nodes into the lowest warps measured slower: the build waits on the
 // gathers of positions and masses, not on idle lanes.)
 template <typename K, bool SPLIT>
-__global__ void __launch_bounds__(kBuildBlock)
+__global__ void __launch_bounds__(build_block<SPLIT>())
 build_fill_kernel(const BuildArgs<K> A) {
-    constexpr int B = kBuildBlock;
-    __shared__ BuildShared<K> S;
+    constexpr int B = build_block<SPLIT>();
+    __shared__ BuildShared<K, B> S;
 
     const uint32_t n = A.n;
     const int t = (int)threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -454,7 +463,7 @@ build_fill_kernel(const BuildArgs<K> A) {
     c.sxx = 0.0f; c.sxy = 0.0f; c.syy = 0.0f;
     c.dm = 0.0; c.dmx = 0.0; c.dmy = 0.0;
     c.local = true;
-    climb<K, true, SPLIT>(A, c, &S, B0);
+    climb<K, B, true, SPLIT>(A, c, &S, B0);
 }
 
 // Second kernel of the split build: one thread per frontier node (a node
@@ -462,10 +471,10 @@ build_fill_kernel(const BuildArgs<K> A) {
 // CTA) continues the climb with the device-scope protocol.  The node's
 // record is read back from the tree arrays the first kernel wrote; no
 // frontier node is large enough for the FP64 path (local nodes hold fewer
-// than kBuildBlock < kFp64MinBodies bodies).  Each climb ends without
+// than kBuildBlockSplit < kFp64MinBodies bodies).  Each climb ends without
 // waiting for any other thread, so a thread may take several entries.
 template <typename K>
-__global__ void __launch_bounds__(kBuildBlock)
+__global__ void __launch_bounds__(kClimbBlock)
 build_climb_kernel(const BuildArgs<K> A) {
     const uint32_t count = *A.frontier_count;
     const uint32_t n = A.n, nm1 = n - 1;
@@ -499,7 +508,7 @@ build_climb_kernel(const BuildArgs<K> A) {
             c.cm = mom.z; c.cx = mom.x; c.cy = mom.y;
             c.lox = box.x; c.loy = box.y; c.hix = box.z; c.hiy = box.w;
         }
-        climb<K, false, false>(A, c, nullptr, 0u);
+        climb<K, kBuildBlockSplit, false, false>(A, c, nullptr, 0u);
     }
 }
 

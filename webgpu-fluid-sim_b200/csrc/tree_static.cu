@@ -88,7 +88,8 @@ static void launch_static(const void* codes, const uint32_t* ids, const float* m
     a.groups = nullptr;
     a.group_count = nullptr;
     a.gmax = 0u;
-    build_fill_kernel<K, false><<<(n + 255) / 256, 256, 0, s>>>(a);
+    constexpr uint32_t B = build_block<false>();
+    build_fill_kernel<K, false><<<(n + B - 1) / B, B, 0, s>>>(a);
 }
 
 }  // namespace bh
