@@ -191,7 +191,12 @@ int sort_passes(const DeviceBuffers& b);
 // tree.cu
 void launch_build_fill(const DeviceBuffers& b, int fp64_levels, cudaStream_t s);
 // Bodies from which the build runs as two kernels (local phase + frontier climb).
-constexpr uint32_t kSplitBuildMin = 1u << 21;
+// Measured crossover (tree stage, B200): 0.8M fused 0.137 / split 0.151 ms, 1.5M
+// equal (0.211), 3M fused 0.371 / split 0.342, 4.2M 0.556 / 0.470.
+#ifndef BH_SPLIT_BUILD_MIN
+#define BH_SPLIT_BUILD_MIN (1u << 21)
+#endif
+constexpr uint32_t kSplitBuildMin = BH_SPLIT_BUILD_MIN;
 bool split_build(uint32_t n);
 void launch_ref_layout(const DeviceBuffers& b, cudaStream_t s);  // group walk: node4/aabb/children/range on request
 void init_bound(const DeviceBuffers& b, cudaStream_t s);
