@@ -151,3 +151,29 @@ def test_velocity_upload_then_other_calls(bh):
     s.sync()
     assert s.download()[2].shape == (3000, 2)
     s.close()
+
+
+def test_velocity_upload_overlap_on_an_ensemble(bh):
+    """The same overlap on an ensemble handle (its tree stages and walk take
+    the per-system paths): bit-equal to waiting for the upload."""
+    cfg = bh.Config(walk="group", softening="plummer", plummerEps=1e-3, mortonDomain="bbox",
+                    integrator="symplectic-euler", deltaTime=5e-5)
+    sizes = [3000, 700, 5000]
+    a = bh.Ensemble(sizes, cfg)
+    b = bh.Ensemble(sizes, cfg)
+    a.setScenarios(None, seed=4)
+    b.setScenarios(None, seed=4)
+    m, p, v = a.download()
+    keep = []
+    for k in range(2):
+        hm, hp, hv = _pinned(m), _pinned(p), _pinned(v * (1.0 + 0.25 * k))
+        keep.append((hm, hp, hv))
+        a.upload(hm, hp, hv)
+        a.step(2)
+        b.upload(hm, hp, hv)
+        b.sync()
+        b.step(2)
+    for x, y in zip(a.download(), b.download()):
+        assert np.array_equal(x, y)
+    a.close()
+    b.close()
