@@ -111,12 +111,12 @@ int bh_update_metadata(bh_sim* sim);
  * checkpoint path).  n must equal the body count.  Any pointer may be NULL
  * to skip that array.  bh_upload is asynchronous for page-locked host
  * memory, which must stay valid until the copies are done (the next
- * bh_sync or bh_download): masses and positions are copied on the handle's
- * stream, velocities on a second copy stream of the handle, ordered after
- * everything enqueued before; the next step's tree stages do not wait for
- * the velocities (they first read them in the walk), every other call orders
- * the handle's stream after them.  bh_download synchronises before
- * returning. */
+ * bh_sync or bh_download): positions are copied on the handle's stream,
+ * masses and then velocities on a second copy stream of the handle, ordered
+ * after everything enqueued before.  The next step's stages before their
+ * first reader (the hierarchy build for the masses, the walk for the
+ * velocities) do not wait for them; every other call orders the handle's
+ * stream after them.  bh_download synchronises before returning. */
 int bh_upload(bh_sim* sim, const float* mass, const float* pos, const float* vel, uint32_t n);
 int bh_download(bh_sim* sim, float* mass, float* pos, float* vel, uint32_t n);
 

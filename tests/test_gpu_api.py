@@ -177,3 +177,29 @@ def test_velocity_upload_overlap_on_an_ensemble(bh):
         assert np.array_equal(x, y)
     a.close()
     b.close()
+
+
+def test_partial_uploads_overlapping_the_step(bh):
+    """Uploads of some arrays only (masses and velocities travel on the copy
+    stream, positions on the handle's stream), each followed by a step:
+    bit-equal to waiting for the upload."""
+    cfg = dict(walk="group", softening="plummer", plummerEps=1e-3, mortonDomain="bbox",
+               integrator="symplectic-euler", deltaTime=1e-3)
+    a = _sim(bh, n=12000, **cfg)
+    b = _sim(bh, n=12000, **cfg)
+    m, p, v = a.download()
+    keep = []
+    patterns = [(m, p, v), (None, None, 0.5 * v), (1.5 * m, None, None), (None, 1.01 * p, None),
+                (m, None, v)]
+    for pm, pp, pv in patterns:
+        arrs = tuple(None if x is None else _pinned(x) for x in (pm, pp, pv))
+        keep.append(arrs)
+        a.upload(*arrs)
+        a.step(1)
+        b.upload(*arrs)
+        b.sync()
+        b.step(1)
+    for x, y in zip(a.download(), b.download()):
+        assert np.array_equal(x, y)
+    a.close()
+    b.close()

@@ -39,17 +39,19 @@ struct bh_sim {
     void* arena = nullptr;
     size_t arena_bytes = 0;
     bool acc_valid = false;
-    // graphs: [0] plain, [1] with event-record nodes at the stage boundaries,
-    // [2] the tree stages alone and [3] the walk alone (the first step after an
-    // upload whose velocities are still being copied, see bh_upload)
-    cudaGraph_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};
-    // Uploaded velocities cross PCIe on copy_stream, ordered after the
-    // stream's earlier work (ev_copy_order); the stream waits on ev_vel before
-    // the next use of the velocities (settle_vel).
+    // graphs: [0] plain, [1] with event-record nodes at the stage boundaries;
+    // for the first step after an upload still being copied (see bh_upload):
+    // [2] the tree stages, [3] the walk, [4] the tree stages up to the sort
+    // without packed leaf records, [5] the build reading masses and positions
+    static constexpr int kGraphs = 6;
+    cudaGraph_t graph[kGraphs] = {};
+    cudaGraphExec_t exec[kGraphs] = {};
+    // Uploaded masses and velocities cross PCIe on copy_stream, ordered after
+    // the stream's earlier work (ev_copy_order); the stream waits on ev_mass /
+    // ev_vel before the next use of those arrays (settle_uploads).
     cudaStream_t copy_stream = nullptr;
-    cudaEvent_t ev_copy_order = nullptr, ev_vel = nullptr;
-    mutable bool vel_pending = false;
+    cudaEvent_t ev_copy_order = nullptr, ev_mass = nullptr, ev_vel = nullptr;
+    mutable bool mass_pending = false, vel_pending = false;
     cudaGraphNode_t ev_node[kMarkers] = {};
     cudaEvent_t markers[kMarkers] = {};
     // profiling
@@ -80,14 +82,23 @@ struct bh_sim {
 
 static thread_local std::string g_err;
 
-// Orders the handle's stream after a velocity upload still in flight on the
-// copy stream.  Every entry point calls it (through BH_HANDLE) before it
-// touches the body buffers, except bh_upload and bh_step, which order the
-// copy themselves.
+// Order the handle's stream after mass / velocity uploads still in flight on
+// the copy stream.  Every entry point calls settle_uploads (through
+// BH_HANDLE) before it touches the body buffers, except bh_upload and
+// bh_step, which order the copies themselves.
+static void settle_mass(const bh_sim* s) {
+    if (!s->mass_pending) return;
+    cudaStreamWaitEvent(s->stream, s->ev_mass, 0);
+    s->mass_pending = false;
+}
 static void settle_vel(const bh_sim* s) {
     if (!s->vel_pending) return;
     cudaStreamWaitEvent(s->stream, s->ev_vel, 0);
     s->vel_pending = false;
+}
+static void settle_uploads(const bh_sim* s) {
+    settle_mass(s);
+    settle_vel(s);
 }
 
 namespace bh {
@@ -100,7 +111,7 @@ namespace bh {
 // refreshes the reference node layout); false for a null handle.
 bool sim_body_view(const bh_sim* s, BodyView* out) {
     if (!s || !out) return false;
-    settle_vel(s);  // callers use the buffers on the handle's stream
+    settle_uploads(s);  // callers use the buffers on the handle's stream
     out->mass = s->b.mass;
     out->pos = s->b.pos;
     out->vel = s->b.vel;
@@ -186,7 +197,7 @@ static int validate_config(bh_sim* s, const bh_config& c) {
 // ---- buffers --------------------------------------------------------------
 
 static void destroy_graphs(bh_sim* s) {
-    for (int v = 0; v < 4; ++v) {
+    for (int v = 0; v < bh_sim::kGraphs; ++v) {
         if (s->exec[v]) cudaGraphExecDestroy(s->exec[v]);
         if (s->graph[v]) cudaGraphDestroy(s->graph[v]);
         s->exec[v] = nullptr;
@@ -254,7 +265,7 @@ static int save_tree(bh_sim* s, uint32_t k) {
 
 static void free_buffers(bh_sim* s) {
     if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);  // no copy into freed memory
-    s->vel_pending = false;
+    s->mass_pending = s->vel_pending = false;
     destroy_graphs(s);
     free_adjoint(s);
     if (s->arena) cudaFree(s->arena);
@@ -407,9 +418,11 @@ static bool needs_bbox(const bh_sim* s) {
     return s->cfg.morton_bits == 64 || s->cfg.morton_domain == BH_DOMAIN_BBOX;
 }
 
-// Tree stages: scratch reset, bbox, Morton encode, sort, build + fill.
+// Tree stages: scratch reset, bbox, Morton encode, sort (the front), then
+// build + fill.  With b.xm null the encode writes no packed leaf records (and
+// reads no masses) and the build reads masses and positions directly.
 template <class Mark>
-static void enqueue_tree_on(bh_sim* s, const DeviceBuffers& b, Mark mark) {
+static void enqueue_tree_front(bh_sim* s, const DeviceBuffers& b, Mark mark) {
     cudaStream_t st = s->stream;
     cudaMemsetAsync(b.scratch, 0, sizeof(bh::StepScratch), st);
     cudaMemsetAsync(b.status, 0, sizeof(uint32_t) * (size_t)b.key_bytes * b.tiles * bh::kRadix, st);
@@ -425,7 +438,12 @@ static void enqueue_tree_on(bh_sim* s, const DeviceBuffers& b, Mark mark) {
     mark(2);
     bh::launch_sort(b, st);
     mark(3);
-    bh::launch_build_fill(b, s->cfg.fp64_levels, st);
+}
+
+template <class Mark>
+static void enqueue_tree_on(bh_sim* s, const DeviceBuffers& b, Mark mark) {
+    enqueue_tree_front(s, b, mark);
+    bh::launch_build_fill(b, s->cfg.fp64_levels, s->stream);
     mark(4);
 }
 
@@ -458,6 +476,11 @@ static int capture_graph(bh_sim* s, int variant) {
     BH_CUDA(s, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     if (variant == 2) {
         enqueue_tree(s, [](int) {});  // symplectic Euler: the step's stages before the walk
+    } else if (variant == 4 || variant == 5) {
+        DeviceBuffers b = s->b;
+        b.xm = nullptr;  // the masses may still be on their way
+        if (variant == 4) enqueue_tree_front(s, b, [](int) {});
+        else bh::launch_build_fill(b, s->cfg.fp64_levels, st);
     } else if (variant == 3) {
         launch_walk_any(s, walk_params(s, bh::kWalkEulerKickDrift));
     } else {
@@ -536,7 +559,7 @@ static int check_device_errors(bh_sim* s) {
 #define BH_HANDLE(s)                                                                        \
     do {                                                                                    \
         BH_HANDLE_NO_SETTLE(s);                                                             \
-        settle_vel(s);                                                                      \
+        settle_uploads(s);                                                                  \
     } while (0)
 
 // ---- lifetime ------------------------------------------------------------------
@@ -613,6 +636,7 @@ static int create_sim(const bh_config* config, const uint32_t* sizes, uint32_t n
         (e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&s->ev_copy_order, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&s->ev_mass, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&s->ev_vel, cudaEventDisableTiming)) != cudaSuccess ||
         (e = bh::sort_init_attributes()) != cudaSuccess) {
         int r = cuda_fail(nullptr, e, "bh_create");
@@ -653,6 +677,7 @@ extern "C" int bh_destroy(bh_sim* s) {
     for (int k = 0; k < kMarkers; ++k)
         if (s->markers[k]) cudaEventDestroy(s->markers[k]);
     if (s->ev_vel) cudaEventDestroy(s->ev_vel);
+    if (s->ev_mass) cudaEventDestroy(s->ev_mass);
     if (s->ev_copy_order) cudaEventDestroy(s->ev_copy_order);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -813,18 +838,25 @@ extern "C" int bh_upload(bh_sim* s, const float* mass, const float* pos, const f
     BH_HANDLE_NO_SETTLE(s);
     if (n != s->b.n) return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_upload: n differs from the body count");
     if (n == 0) return BH_OK;
-    if (mass) BH_CUDA(s, cudaMemcpyAsync(s->b.mass, mass, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
     if (pos) BH_CUDA(s, cudaMemcpyAsync(s->b.pos, pos, 8 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
-    if (vel) {
+    if (mass || vel) {
         // On the copy stream, after everything enqueued so far on the handle's
-        // stream (so after the mass and position copies, and after any step
-        // still reading or writing the velocities); the next step's tree
-        // stages do not wait for it (step_once), every other call does.
+        // stream (so after the position copy, and after any step still
+        // reading the masses or reading or writing the velocities): masses,
+        // then velocities.  The next step's stages before their first reader
+        // do not wait for them (step_once); every other call does.
         BH_CUDA(s, cudaEventRecord(s->ev_copy_order, s->stream));
         BH_CUDA(s, cudaStreamWaitEvent(s->copy_stream, s->ev_copy_order, 0));
-        BH_CUDA(s, cudaMemcpyAsync(s->b.vel, vel, 8 * (size_t)n, cudaMemcpyHostToDevice, s->copy_stream));
-        BH_CUDA(s, cudaEventRecord(s->ev_vel, s->copy_stream));
-        s->vel_pending = true;
+        if (mass) {
+            BH_CUDA(s, cudaMemcpyAsync(s->b.mass, mass, 4 * (size_t)n, cudaMemcpyHostToDevice, s->copy_stream));
+            BH_CUDA(s, cudaEventRecord(s->ev_mass, s->copy_stream));
+            s->mass_pending = true;
+        }
+        if (vel) {
+            BH_CUDA(s, cudaMemcpyAsync(s->b.vel, vel, 8 * (size_t)n, cudaMemcpyHostToDevice, s->copy_stream));
+            BH_CUDA(s, cudaEventRecord(s->ev_vel, s->copy_stream));
+            s->vel_pending = true;
+        }
     }
     if (mass || pos) s->acc_valid = false;
     return BH_OK;
@@ -846,27 +878,40 @@ extern "C" int bh_download(bh_sim* s, float* mass, float* pos, float* vel, uint3
 
 static int step_once(bh_sim* s) {
     const bool kdk = s->cfg.integrator == BH_INTEGRATOR_LEAPFROG_KDK;
+    cudaEvent_t* ev = prof_slot(s);
+    const bool overlap = (s->mass_pending || s->vel_pending) && !kdk && !ev && s->cfg.use_graphs;
+    if (!overlap) settle_uploads(s);  // leapfrog reads both at once (force evaluation, opening kick)
     if (kdk && !s->acc_valid) {
         enqueue_forces(s, [](int) {});  // first force evaluation of a leapfrog run
         s->acc_valid = true;
     }
-    cudaEvent_t* ev = prof_slot(s);
-    if (s->vel_pending && !kdk && !ev && s->cfg.use_graphs) {
-        // The last upload's velocities are still crossing PCIe on the copy
-        // stream; the walk is their first reader, so the tree stages run
-        // meanwhile (the same kernels in the same order as the whole-step graph).
-        for (int v = 2; v < 4; ++v)
+    if (overlap) {
+        // The last upload's masses and velocities are still crossing PCIe on
+        // the copy stream (masses first).  The build is the masses' first
+        // reader and the walk the velocities', so the stages before them run
+        // meanwhile: the same kernels in the same order as the whole-step
+        // graph, except that with masses pending the encode writes no packed
+        // leaf records and the build gathers masses and positions instead
+        // (the same values).
+        const bool m = s->mass_pending;
+        const int need[3] = {m ? 4 : 2, m ? 5 : 3, 3};
+        for (int v : need)
             if (!s->exec[v]) {
                 int rc = capture_graph(s, v);
                 if (rc != BH_OK) return rc;
             }
-        BH_CUDA(s, cudaGraphLaunch(s->exec[2], s->stream));
+        if (m) {
+            BH_CUDA(s, cudaGraphLaunch(s->exec[4], s->stream));
+            settle_mass(s);
+            BH_CUDA(s, cudaGraphLaunch(s->exec[5], s->stream));
+        } else {
+            BH_CUDA(s, cudaGraphLaunch(s->exec[2], s->stream));
+        }
         settle_vel(s);
         BH_CUDA(s, cudaGraphLaunch(s->exec[3], s->stream));
         s->acc_valid = false;
         return BH_OK;
     }
-    settle_vel(s);
     if (s->cfg.use_graphs) {
         const int v = ev ? 1 : 0;
         if (!s->exec[v]) {
