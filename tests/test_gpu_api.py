@@ -179,14 +179,15 @@ def test_velocity_upload_overlap_on_an_ensemble(bh):
     b.close()
 
 
-def test_partial_uploads_overlapping_the_step(bh):
+@pytest.mark.parametrize("n", [1, 2, 300, 12000])
+def test_partial_uploads_overlapping_the_step(bh, n):
     """Uploads of some arrays only (masses and velocities travel on the copy
     stream, positions on the handle's stream), each followed by a step:
-    bit-equal to waiting for the upload."""
+    bit-equal to waiting for the upload, down to one and two bodies."""
     cfg = dict(walk="group", softening="plummer", plummerEps=1e-3, mortonDomain="bbox",
                integrator="symplectic-euler", deltaTime=1e-3)
-    a = _sim(bh, n=12000, **cfg)
-    b = _sim(bh, n=12000, **cfg)
+    a = _sim(bh, n=n, **cfg)
+    b = _sim(bh, n=n, **cfg)
     m, p, v = a.download()
     keep = []
     patterns = [(m, p, v), (None, None, 0.5 * v), (1.5 * m, None, None), (None, 1.01 * p, None),
