@@ -14,8 +14,9 @@
 //    ballot multisplit (stable: item-major, lane-minor = memory order),
 //    publishes its per-digit counts, stages the tile in shared memory in
 //    digit order, and then resolves its global offsets by a decoupled
-//    look-back over the tiles before it, several tiles per round trip.  The look-back spin is bounded; on giving up it raises
-//    kErrLookbackSpin instead of hanging.
+//    look-back over the tiles before it, several tiles per round trip.  The
+//    look-back spin is bounded; on giving up it raises kErrLookbackSpin
+//    instead of hanging.
 //  - Staged keys and ids are written out in runs, so global stores are
 //    contiguous per digit.
 //  - Pass 0 does not read ids: it writes the identity permutation of
