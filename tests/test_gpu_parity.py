@@ -154,9 +154,9 @@ def test_split_build_matches_oracle_beyond_2m(bh, orc, cfg):
     # the frontier nodes it leaves; both node layouts against the oracle.
     n = (1 << 21) + 4097
     sim = make_sim(bh, n, "gaussian-mixture", seed=3, **cfg)
-    # bbox, encode, sort passes, build (2 kernels), walk
-    assert sim.kernels_per_step() == (1 + 1 + 8 + 2 + 1 if cfg.get("mortonBits") == 64
-                                      else 1 + 1 + 4 + 2 + 1)
+    # reset, bbox, encode, sort passes, build (2 kernels), walk
+    assert sim.kernels_per_step() == (1 + 1 + 1 + 8 + 2 + 1 if cfg.get("mortonBits") == 64
+                                      else 1 + 1 + 1 + 4 + 2 + 1)
     mass, pos, vel = sim.download()
     sim.computeAccelerations()
     t = sim.tree()
@@ -198,7 +198,7 @@ def test_profile_and_kernel_count(bh):
     ms, steps = sim.profile_end()
     assert steps == 5
     assert all(v >= 0 for v in ms.values()) and ms["walk"] > 0
-    assert sim.kernels_per_step() == 1 + 4 + 1 + 1  # encode, 4 sort passes, build+fill, walk
+    assert sim.kernels_per_step() == 1 + 1 + 4 + 1 + 1  # reset, encode, 4 sort passes, build+fill, walk
     # a second profiling window on the same captured graph
     sim.profile_begin(3)
     sim.step(3)

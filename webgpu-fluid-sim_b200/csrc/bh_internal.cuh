@@ -185,6 +185,7 @@ void launch_kick_drift(const DeviceBuffers& b, float dt, cudaStream_t s);
 void launch_bbox_ensemble(const DeviceBuffers& b, cudaStream_t s);
 void launch_encode_ensemble(const DeviceBuffers& b, cudaStream_t s);
 // sort.cu
+void launch_zero_step(const DeviceBuffers& b, cudaStream_t s);  // scratch + sort status
 void launch_sort(const DeviceBuffers& b, cudaStream_t s);
 cudaError_t sort_init_attributes();
 int sort_passes(const DeviceBuffers& b);

@@ -424,8 +424,7 @@ static bool needs_bbox(const bh_sim* s) {
 template <class Mark>
 static void enqueue_tree_front(bh_sim* s, const DeviceBuffers& b, Mark mark) {
     cudaStream_t st = s->stream;
-    cudaMemsetAsync(b.scratch, 0, sizeof(bh::StepScratch), st);
-    cudaMemsetAsync(b.status, 0, sizeof(uint32_t) * (size_t)b.key_bytes * b.tiles * bh::kRadix, st);
+    bh::launch_zero_step(b, st);  // scratch record + sort look-back status
     mark(1);
     if (b.num_systems > 0) {
         cudaMemsetAsync(b.sys_bbox, 0, sizeof(uint32_t) * 4 * (size_t)b.num_systems, st);
@@ -1400,6 +1399,7 @@ extern "C" int bh_kernels_per_step(bh_sim* s, uint32_t* out) {
     if (!s || !out) return fail(s, BH_ERR_INVALID_ARGUMENT, "null argument");
     uint32_t k = 0;
     if (s->cfg.integrator == BH_INTEGRATOR_LEAPFROG_KDK) k += 1;  // kick + drift
+    k += 1;                                                         // scratch reset
     if (needs_bbox(s) || s->b.num_systems) k += 1;                 // bbox (per system)
     k += 1;                                                         // encode
     k += (uint32_t)bh::sort_passes(s->b);                          // sort passes

@@ -332,6 +332,31 @@ __global__ void __launch_bounds__(256) kick_drift_kernel(float2* __restrict__ po
     }
 }
 
+// ---- per-step reset ---------------------------------------------------------
+// Zeroes the step's scratch record and the sort's look-back status in one
+// launch (in a captured step, two memset nodes cost more than these writes).
+static_assert(sizeof(StepScratch) % 4 == 0, "scratch is cleared in 4-byte words");
+__global__ void __launch_bounds__(256) zero_step_kernel(uint32_t* __restrict__ scratch, uint32_t words,
+                                                        uint4* __restrict__ status, size_t quads) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = t; i < words; i += stride) scratch[i] = 0u;
+    for (size_t i = t; i < quads; i += stride) status[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+void launch_zero_step(const DeviceBuffers& b, cudaStream_t s) {
+    // status: key_bytes passes x tiles x 256 words, a multiple of 16 bytes,
+    // 256-byte aligned in the arena like the scratch record
+    const size_t quads = (size_t)b.key_bytes * b.tiles * kRadix / 4;
+    const uint32_t words = (uint32_t)(sizeof(StepScratch) / 4);
+    const size_t work = quads > words ? quads : words;
+    size_t blocks = (work + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    zero_step_kernel<<<(unsigned)blocks, 256, 0, s>>>(reinterpret_cast<uint32_t*>(b.scratch), words,
+                                                      reinterpret_cast<uint4*>(b.status), quads);
+}
+
 void launch_kick_drift(const DeviceBuffers& b, float dt, cudaStream_t s) {
     if (b.n == 0) return;
     int blocks = (int)((b.n + 255) / 256);
