@@ -17,15 +17,22 @@ Own arm (default):
              in the step graph during the timed steps.
   cpu_baseline  the oracle (C restatement, OpenMP, all host threads) on a
              bounded sample of the same workload.
+  secondary  the 16.8M-body Gaussian-mixture point of the metric with the
+             same figures (value, stages, roofline, e2e, force error,
+             cpu_baseline).
 Reference arm (--impl reference): the reference's own pipeline logic on the
 host cores: its WGSL compute shaders mechanically translated to C++
 (oracle/_ref, built where the reference checkout exists), all host threads;
 if that build is absent, the oracle port.  The WGSL itself needs a WebGPU
-device, which this machine lacks.
+device, which this machine lacks.  That arm imports nothing from the engine
+package: its inputs come from the oracle's generators.
 
-Multi-GPU (torchrun): every rank simulates its own independently seeded copy
-of the workload (weak scaling, no collective on the data path); the timed
-region is bracketed by barriers and the max over ranks is reported.
+Multi-GPU (torchrun): by default one system on all ranks (--shard: every
+rank builds the same tree, walks its range of sorted slots, and the ranks
+all-gather the updated bodies once per step: strong scaling); --replicas
+runs an independently seeded copy per rank instead (weak scaling, no
+collective).  The timed region is bracketed by barriers and the max over
+ranks is reported.
 """
 from __future__ import annotations
 
@@ -47,9 +54,38 @@ PKG = "webgpu-fluid-sim_b200"
 DEFAULT_WORKLOAD = "colliding-disks-800k"
 FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes (read + write) of one launch of the dominant kernel (the walk),
-# from one ncu capture of the same workload
-# (profiles/walk_group_build_fill_onesweep_colliding-disks-800k.md).
+# from one ncu capture of the same workload.
 NCU_WALK_TRAFFIC_BYTES = {"colliding-disks-800k": 44.16e6}
+# Algorithmic HBM bytes per body and step of the stream stages: encode =
+# position 8 + mass 4 read, key 4|8 + packed leaf record 16 written; sort =
+# first pass key read + key and id written, later passes key and id read and
+# written; build = key 4|8 + id 4 + leaf gather 16 read, leaf record 16 +
+# parents 8 + one 64-B internal-node record written.
+STREAM_BYTES = {4: {"morton": 8 + 4 + 4 + 16, "sort": 12 + 3 * 16, "tree": 4 + 4 + 16 + 16 + 8 + 64},
+                8: {"morton": 8 + 4 + 8 + 16, "sort": 20 + 7 * 24, "tree": 8 + 4 + 16 + 16 + 8 + 64}}
+# Plain parameters of the workloads for the CPU legs, which must not import
+# the engine package: body count, scenario and the oracle's parameters
+# (oracle.params keywords).  tests/test_bench.py checks them against the
+# package's WORKLOADS.
+def _orc_params(theta, eps, dt, bits, domain, integrator):
+    return dict(G=1.0, dt=dt, theta=theta, softening="plummer", plummer_eps=eps,
+                morton_bits=bits, morton_domain=domain, integrator=integrator, leaf_size=8,
+                walk="group", multipole=2, bodies_per_lane=2)
+
+
+REF_WORKLOADS = {
+    "uniform-disk-16k": dict(n=16384, scenario="uniform-disk-kepler",
+                             oracle=_orc_params(0.7, 1e-3, 1e-4, 32, "bbox", "leapfrog-kdk")),
+    "colliding-disks-800k": dict(n=800_000, scenario="colliding-disks",
+                                 oracle=_orc_params(0.5, 1e-3, 5e-5, 32, "bbox",
+                                                    "symplectic-euler")),
+    "gaussian-mixture-16m": dict(n=16_777_216, scenario="gaussian-mixture",
+                                 oracle=_orc_params(0.5, 1e-4, 1e-5, 64, "fixed2000",
+                                                    "symplectic-euler")),
+    "gaussian-mixture-4m": dict(n=4_194_304, scenario="gaussian-mixture",
+                                oracle=_orc_params(0.5, 1e-4, 1e-5, 64, "fixed2000",
+                                                   "symplectic-euler")),
+}
 
 
 def parse():
@@ -69,8 +105,11 @@ def parse():
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-render", action="store_true")
+    ap.add_argument("--no-exact-walk", action="store_true")
     ap.add_argument("--shard", action="store_true",
-                    help="one system on all ranks (strong scaling) instead of one per rank")
+                    help="one system on all ranks (strong scaling); the default with N > 1")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with N > 1: an independently seeded copy of the workload per rank")
     return ap.parse_args()
 
 
@@ -110,12 +149,88 @@ def adjoint_cost(pkg, device: int, n: int = 65536, steps: int = 200, every: int 
             "timing": "host wall clock around synchronised calls, best of 3"}
 
 
-def secondary_16m(pkg, device: int, steps: int = 5) -> dict:
-    """The 16.8M-body Gaussian-mixture point of the metric (64-bit keys)."""
+def walk_roofline(cfg, walk_ms: float, multi_inter: int, body_inter: int, visits: int,
+                  sm_max_mhz, traffic=None) -> dict:
+    """Roofline of the walk: algorithmic FP32 flops per launch over its time,
+    against the nominal FP32 FMA rate.  Flops: 16 per monopole interaction
+    (2 sub, 3 for d^2+eps^2, 4 for rsqrt, 2 for inv^3, 1 for m inv^3, 4 for
+    two FMA) and 35 per monopole + quadrupole interaction (the 16 plus Q'r 6,
+    r.Q'r 3, inv^5 1, 2.5 r.Q'r inv^7 3, two extra FMA 4, one add 2), times
+    the interactions an instrumented launch of the same walk counts."""
+    quad = cfg.walk == "group" and cfg.multipole >= 2
+    flops = (35.0 if quad else 16.0) * multi_inter + 16.0 * body_inter
+    mhz = sm_max_mhz or 1965.0
+    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12  # nominal FMA peak at max clock
+    achieved = flops / (walk_ms / 1e3) / 1e12
+    return {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+            "frac": achieved / fp32_peak, "traffic": traffic,
+            "traffic_unit": "bytes per launch (ncu dram read + write)",
+            "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2 x max SM clock);"
+                           " no measured FP32 peak exists for this pool",
+            "kernel": "walk", "kernel_ms": walk_ms,
+            "multipole_interactions_per_step": multi_inter,
+            "body_interactions_per_step": body_inter,
+            "node_visits_per_step": visits, "flops_per_step": flops}
+
+
+def stream_rooflines(stages: dict, n: int, key_bytes: int, hbm_gbs: float) -> dict:
+    """HBM fraction of each stream stage: its algorithmic bytes over its time."""
+    out = {}
+    for stage, per_body in STREAM_BYTES[key_bytes].items():
+        ms = stages.get(stage, 0.0)
+        if ms <= 0.0:
+            continue
+        gbs = per_body * n / (ms / 1e3) / 1e9
+        out[stage] = {"bytes_per_body": per_body, "ms": ms, "achieved_gbs": gbs,
+                      "peak_gbs": hbm_gbs, "frac": gbs / hbm_gbs}
+    return out
+
+
+def e2e_rate(sim, step, n: int, steps: int, ext, barrier=lambda: None, dist=None, units=None):
+    """The metric through the public API with host buffers: per step, upload
+    masses, positions and velocities from page-locked memory, one step,
+    download positions and velocities into page-locked memory; CUDA events on
+    the engine's stream around the whole loop."""
+    import torch
+    mass, pos, vel = sim.download()
+    h_mass = torch.from_numpy(mass).pin_memory()
+    h_pos = torch.from_numpy(pos).pin_memory()
+    h_vel = torch.from_numpy(vel).pin_memory()
+    o_pos = torch.empty_like(h_pos).pin_memory()
+    o_vel = torch.empty_like(h_vel).pin_memory()
+    sim.upload(h_mass, h_pos, h_vel)
+    step(1)
+    sim.download_into(None, o_pos, o_vel)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for _ in range(steps):
+        sim.upload(h_mass, h_pos, h_vel)
+        step(1)
+        sim.download_into(None, o_pos, o_vel)  # synchronises the stream
+    e1.record(ext)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=torch.device("cuda", sim.device))
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return {"value": (units or n) * steps / (float(t.item()) / 1e3), "unit": "body-steps/s",
+            "h2d_bytes_per_step": int(h_mass.nbytes + h_pos.nbytes + h_vel.nbytes),
+            "d2h_bytes_per_step": int(o_pos.nbytes + o_vel.nbytes), "steps": steps}
+
+
+def secondary_16m(pkg, device: int, steps: int = 5, e2e_steps: int = 3, sm_max_mhz=None,
+                  hbm_gbs: float = 6650.0, with_cpu: bool = True) -> dict:
+    """The 16.8M-body Gaussian-mixture point of the metric (64-bit keys), with
+    the same figures as the headline: device rate, stages, walk roofline and
+    stream-stage HBM fractions, e2e through the public API, FP64 force error
+    on 1,024 bodies and the reference's CPU rate on a bounded sample."""
     import torch
     wl = pkg.WORKLOADS["gaussian-mixture-16m"]
+    n = wl["n"]
     sim = pkg.Simulation(wl["config"], device=device)
-    sim.setNumBodies(wl["n"])
+    sim.setNumBodies(n)
     sim.setScenario(wl["scenario"], 1)
     tune = sim.autotune(2)
     for _ in range(3):
@@ -131,15 +246,66 @@ def secondary_16m(pkg, device: int, steps: int = 5) -> dict:
     sim.sync()
     stage_ms, rec = sim.profile_end()
     ms = e0.elapsed_time(e1) / steps
-    mass, pos, _ = sim.download()
-    acc = sim.computeAccelerations()
-    med, p99, ns = force_error_vs_fp64(acc, mass, pos, wl["config"], nsample=64)
+    stages = {k: v / max(rec, 1) for k, v in stage_ms.items()}
+    cfg = sim.config
+    visits, multi, body = sim.walk_stats()
+    acc = sim.read_buffer("acc", np.float32, 2 * n).reshape(n, 2)
+    ferr = sim.forceError(acc, nsample=1024, seed=1)
+    e2e = e2e_rate(sim, sim.step, n, e2e_steps, ext)
+    kps = sim.kernels_per_step()
     sim.close()
-    return {"workload": "gaussian-mixture-16m", "bodies": wl["n"], "value": wl["n"] / (ms / 1e3),
-            "unit": "body-steps/s", "ms_per_step": ms,
+    out = {"workload": "gaussian-mixture-16m", "bodies": n, "metric": "body-steps/s",
+           "value": n / (ms / 1e3), "unit": "body-steps/s", "ms_per_step": ms, "steps": steps,
+           "stages_ms": stages,
+           "roofline": walk_roofline(cfg, stages["walk"], multi, body, visits, sm_max_mhz),
+           "stream_stages": stream_rooflines(stages, n, 8, hbm_gbs),
+           "force_error_vs_fp64": ferr, "e2e": e2e, "autotune": tune,
+           "gpu_launches": kps * steps,
+           "config": {"theta": cfg.bhTheta, "softening": f"plummer {cfg.plummerEps}",
+                      "dt": cfg.deltaTime, "integrator": cfg.integrator,
+                      "morton_bits": cfg.mortonBits, "bodies_per_lane": cfg.bodiesPerLane,
+                      "leaf_size": cfg.leafSize},
+           "l2": "working set ~3 GB > L2 (no flush needed)"}
+    if with_cpu:
+        out["cpu_baseline"] = reference_baseline(REF_WORKLOADS["gaussian-mixture-16m"], 20.0)
+    return out
+
+
+def exact_walk_cost(pkg, device: int, steps: int = 10) -> dict:
+    """The reference-semantics walk (walk_mode exact: every body visits the
+    nodes of barnes_hut.wgsl:48-111's per-body monopole DFS, leaf size 1) on
+    the headline workload, with its FP64 force error."""
+    import torch
+    wl = pkg.WORKLOADS["colliding-disks-800k"]
+    n = wl["n"]
+    cfg = dataclasses.replace(wl["config"], walk="exact", leafSize=1)
+    sim = pkg.Simulation(cfg, device=device)
+    sim.setNumBodies(n)
+    sim.setScenario(wl["scenario"], 1)
+    for _ in range(3):
+        sim.step(1)
+    sim.sync()
+    ext = torch.cuda.ExternalStream(sim.getBuffers().stream, device=torch.device("cuda", device))
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=torch.device("cuda", device))
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    sim.profile_begin(steps)
+    with torch.cuda.stream(ext):
+        for i in range(steps):
+            flush.zero_()
+            starts[i].record(ext)
+            sim.step(1)
+            ends[i].record(ext)
+    sim.sync()
+    stage_ms, rec = sim.profile_end()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / steps
+    acc = sim.computeAccelerations()
+    ferr = sim.forceError(acc, nsample=1024, seed=2)
+    sim.close()
+    return {"workload": "colliding-disks-800k", "walk": "exact (reference per-body walk)",
+            "value": n / (ms / 1e3), "unit": "body-steps/s", "ms_per_step": ms,
             "stages_ms": {k: v / max(rec, 1) for k, v in stage_ms.items()},
-            "force_error_vs_fp64": {"median": med, "p99": p99, "sample": ns}, "autotune": tune,
-            "l2": "working set 3 GB > L2"}
+            "force_error_vs_fp64": ferr}
 
 
 def ensemble_cost(pkg, device: int, systems: int = 1024, steps: int = 100,
@@ -386,51 +552,64 @@ def force_error_vs_fp64(acc, mass, pos, cfg, nsample=256, seed=0):
     return float(np.median(errs)), float(np.percentile(errs, 99)), int(idx.size)
 
 
-def reference_baseline(pkg, wl, seconds_budget=20.0):
+def _oracle():
+    d = os.path.join(ROOT, "oracle")
+    if d not in sys.path:
+        sys.path.insert(0, d)
+    import oracle as orc
+    return orc
+
+
+def reference_baseline(wp: dict, seconds_budget=20.0):
     """The reference's own shader logic (oracle/_ref: a mechanical C++
     translation of lbvh.wgsl + barnes_hut.wgsl, independent stages on all host
-    threads) on the workload's bodies, theta and dt.  The reference knows only
-    its own softening, eps = epsMult sqrt(G max(m1, m2) dt); epsMult is set so
-    that eps equals the workload's Plummer eps at the median body mass."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as orc
+    threads) on the workload's bodies, theta and dt.  The bodies come from the
+    oracle's generator (one PCG32 stream per body: the workload's distribution
+    and size).  The reference knows only its own softening, eps = epsMult
+    sqrt(G max(m1, m2) dt); epsMult is set so that eps equals the workload's
+    Plummer eps at the median body mass.  Up to a million bodies every step
+    runs whole; above, the walk (velocity step) runs on every k-th sorted
+    slot and its time is scaled by k, the other stages run whole."""
+    orc = _oracle()
     if not orc.ref_available():
         return None
-    cfg = wl["config"]
-    n = wl["n"]
-    mass, pos, vel, _ = pkg.generate_scenario(wl["scenario"], n, 1, cfg.gravConstant)
+    op = wp["oracle"]
+    n, G, dt = wp["n"], op["G"], op["dt"]
+    mass, pos, vel, _ = orc.generate_per_body(wp["scenario"], n, 1, G)
     m_med = float(np.median(mass))
-    eps_mult = float(cfg.plummerEps / np.sqrt(cfg.gravConstant * m_med * cfg.deltaTime))
-    kw = dict(G=cfg.gravConstant, dt=cfg.deltaTime, eps_mult=eps_mult, theta=cfg.bhTheta,
-              parallel=True)
-    t0 = time.perf_counter()
-    orc.ref_run(mass, pos, vel, steps=1, **kw)  # warm-up and size the sample
-    one = time.perf_counter() - t0
-    steps = int(max(1, min(50, seconds_budget / max(one, 1e-3))))
-    t0 = time.perf_counter()
-    orc.ref_run(mass, pos, vel, steps=steps, **kw)
-    el = time.perf_counter() - t0
+    eps_mult = float(op["plummer_eps"] / np.sqrt(G * m_med * dt))
+    stride = 1 if n <= 1_000_000 else max(1, n // 250_000)
+    kw = dict(G=G, dt=dt, eps_mult=eps_mult, theta=op["theta"], walk_stride=stride)
+    one = orc.ref_run_timed(mass, pos, vel, steps=1, **kw)  # warm-up and size the sample
+    per_step = sum(one.values()) + one["vel_step"] * (stride - 1)
+    steps = int(max(1, min(50, seconds_budget / max(per_step, 1e-3))))
+    st = orc.ref_run_timed(mass, pos, vel, steps=steps, **kw)
+    el = st["morton"] + st["sort"] + st["build_fill"] + stride * st["vel_step"] + st["pos_step"]
     threads = orc.ref_threads()
+    walk = ("the whole walk" if stride == 1 else
+            f"the walk timed on every {stride}th sorted slot and scaled by {stride}")
     return {"value": n * steps / el, "unit": "body-steps/s", "cores": threads, "kind": "reference",
-            "sample": f"{steps} steps of the full {n}-body workload (reference WGSL logic "
-                      f"translated to C++, fixed 2000-unit Morton domain, per-body monopole walk, "
-                      f"epsMult {eps_mult:.1f}, {threads} OpenMP threads; fill serial)"}
+            "stages_s_per_step": {k: v / steps for k, v in st.items()}, "walk_stride": stride,
+            "sample": f"{steps} steps of the {n}-body workload, {walk} (reference WGSL logic "
+                      f"translated to C++: the reference's fixed 2000-unit Morton domain "
+                      f"(lbvh.wgsl:49-57), so the workload's bodies share few grid cells; "
+                      f"per-body monopole walk; epsMult {eps_mult:.1f}; {threads} OpenMP threads; "
+                      f"fill serial; bodies from the oracle's generator)"}
 
 
-def cpu_baseline(pkg, wl, seconds_budget=20.0):
+def cpu_baseline(wp: dict, seconds_budget=20.0):
     """The reference's own logic when it was built here, else the oracle port."""
-    ref = reference_baseline(pkg, wl, seconds_budget)
-    return ref if ref is not None else port_baseline(pkg, wl, seconds_budget)
+    ref = reference_baseline(wp, seconds_budget)
+    return ref if ref is not None else port_baseline(wp, seconds_budget)
 
 
-def port_baseline(pkg, wl, seconds_budget=20.0):
+def port_baseline(wp: dict, seconds_budget=20.0):
     """The oracle (C restatement, OpenMP) on a bounded sample of the workload."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as orc
-    cfg = wl["config"]
-    n = wl["n"]
-    mass, pos, vel, _ = pkg.generate_scenario(wl["scenario"], n, 1, cfg.gravConstant)
-    st = orc.State(orc.params_from_config(cfg), mass, pos, vel)
+    orc = _oracle()
+    op = wp["oracle"]
+    n = wp["n"]
+    mass, pos, vel, _ = orc.generate_per_body(wp["scenario"], n, 1, op["G"])
+    st = orc.State(orc.params(**op), mass, pos, vel)
     threads = orc.load().orc_max_threads()
     st.step(1)  # first step includes the initial force evaluation of the leapfrog
     steps, t0 = 0, time.perf_counter()
@@ -442,26 +621,28 @@ def port_baseline(pkg, wl, seconds_budget=20.0):
             break
     return {"value": n * steps / el, "unit": "body-steps/s", "cores": threads, "kind": "port",
             "sample": f"{steps} steps of the full {n}-body workload after 1 warm-up step "
-                      f"(oracle C restatement, same algorithm as the engine: {cfg.walk} walk, "
+                      f"(oracle C restatement, same algorithm as the engine: {op['walk']} walk, "
                       f"{threads} OpenMP threads)"}
 
 
 # ---------------------------------------------------------------- reference arm
 
 def run_reference(args):
+    """The reference arm: rank 0 alone times the reference's own pipeline
+    logic on the host cores; nothing of the engine package is imported."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    pkg = load_pkg()
-    wl = pkg.WORKLOADS[args.workload]
-    # Each step is a bounded sample: the full workload for one step.
+    wp = REF_WORKLOADS[args.workload]
+    # Each step is a bounded sample of the workload, sized so the whole
+    # --steps K --warmup W run stays within a few minutes.
     budget = max(10.0, 120.0 / max(args.steps + args.warmup, 1))
-    cb = cpu_baseline(pkg, wl, seconds_budget=budget)
+    cb = cpu_baseline(wp, seconds_budget=budget)
     line = {"impl": "reference", "metric": "body-steps/s", "value": cb["value"],
             "unit": "body-steps/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG32)",
-            "config": {"workload": args.workload, "bodies": wl["n"]},
+            "config": {"workload": args.workload, "bodies": wp["n"]},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "body-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -498,7 +679,9 @@ def run_own(args):
         cfg = dataclasses.replace(cfg, bodiesPerLane=bpl, leafSize=leaf)
         args.no_autotune = True
     sharded = None
-    if args.shard:
+    # With several ranks the default is the single system sharded over them
+    # (the path's own exchange step); --replicas opts out.
+    if args.shard or (world > 1 and not args.replicas):
         # One system on all ranks: rank 0 picks the walk shape, everyone uses it
         # (the ranks must build identical trees and groups).
         tune = None
@@ -577,73 +760,28 @@ def run_own(args):
 
     # ---- walk statistics + force error (untimed) ----
     visits, multi_inter, body_inter = sim.walk_stats()
-    mass, pos, vel = sim.download()
     acc = sim.read_buffer("acc", np.float32, 2 * n).reshape(n, 2)
-    med_err, p99_err, nsamp = force_error_vs_fp64(acc, mass, pos, cfg)
+    ferr = sim.forceError(acc, nsample=2048, seed=0) if rank == 0 else None
 
     # ---- e2e through the public API with host buffers ----
-    E = args.e2e_steps
-    h_mass = torch.from_numpy(mass).pin_memory()
-    h_pos = torch.from_numpy(pos).pin_memory()
-    h_vel = torch.from_numpy(vel).pin_memory()
-    o_pos = torch.empty_like(h_pos).pin_memory()
-    o_vel = torch.empty_like(h_vel).pin_memory()
-    sim.upload(h_mass, h_pos, h_vel)
-    step(1)
-    sim.download_into(None, o_pos, o_vel)
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(ext)
-    for _ in range(E):
-        sim.upload(h_mass, h_pos, h_vel)
-        step(1)
-        sim.download_into(None, o_pos, o_vel)  # synchronises the stream
-    e1.record(ext)
-    e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = units * E / (float(t.item()) / 1e3)
+    e2e = e2e_rate(sim, step, n, args.e2e_steps, ext, barrier, dist, units)
 
     out = None
     if rank == 0:
-        import ctypes  # noqa: F401
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         except OSError:
             pass
-        # dominant kernel: the walk.  Algorithmic FP32 flops per launch:
-        # 16 per monopole interaction (2 sub, 3 for d^2+eps^2, 4 for rsqrt,
-        # 2 for inv^3, 1 for m inv^3, 4 for two FMA) and 35 per
-        # monopole + quadrupole interaction (the 16 plus Q'r 6, r.Q'r 3,
-        # inv^5 1, 2.5 r.Q'r inv^7 3, two extra FMA 4, one add 2) x the
-        # interactions counted by an instrumented launch of the same walk.
-        walk_ms = stage_ms["walk"] / max(recorded, 1)
-        quad = cfg.walk == "group" and cfg.multipole >= 2
-        flops = (35.0 if quad else 16.0) * multi_inter + 16.0 * body_inter
-        sm_mhz = clk.get("sm_max_mhz") or 1965.0
-        fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # nominal FMA peak at max clock
-        achieved = flops / (walk_ms / 1e3) / 1e12
-        roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                    "frac": achieved / fp32_peak,
-                    "traffic": NCU_WALK_TRAFFIC_BYTES.get(args.workload),
-                    "traffic_unit": "bytes per launch (ncu dram read + write)",
-                    "peak_source": "nominal FP32 FMA rate (148 SMs x 128 lanes x 2 x max SM clock);"
-                                   " no measured FP32 peak exists for this pool",
-                    "kernel": "walk", "kernel_ms": walk_ms,
-                    "multipole_interactions_per_step": multi_inter,
-                    "body_interactions_per_step": body_inter,
-                    "node_visits_per_step": visits,
-                    "flops_per_step": flops}
+        # dominant kernel: the walk
         stages = {k: v / max(recorded, 1) for k, v in stage_ms.items()}
+        roofline = walk_roofline(cfg, stages["walk"], multi_inter, body_inter, visits,
+                                 clk.get("sm_max_mhz"), NCU_WALK_TRAFFIC_BYTES.get(args.workload))
         hbm = peaks.get("hbm_gbs", 6650.0)
         kps = sim.kernels_per_step()
         cb = None
         if not args.no_cpu_baseline and world == 1:  # the CPU baseline runs at N = 1 only
-            cb = cpu_baseline(pkg, wl)
+            cb = cpu_baseline(REF_WORKLOADS[args.workload])
         out = {
             "metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world,
             "steps": K, "warmup": args.warmup, "ms_per_step": step_ms_max / K,
@@ -662,11 +800,13 @@ def run_own(args):
                        "l2": "flushed between timed steps (256 MB write, outside the events)"},
             "roofline": roofline,
             "stages_ms": stages,
+            "stream_stages": stream_rooflines(stages, n, 8 if cfg.mortonBits == 64 else 4, hbm),
             "hbm_peak_gbs": hbm,
-            "force_error_vs_fp64": {"median": med_err, "p99": p99_err, "sample": nsamp},
+            "hbm_peak_source": ("MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
+                                else "fallback 6650 GB/s (no measured peaks file)"),
+            "force_error_vs_fp64": ferr,
             "cpu_baseline": cb,
-            "e2e": {"value": e2e_value, "unit": "body-steps/s", "h2d_bytes_per_step": 20 * n,
-                    "d2h_bytes_per_step": 16 * n, "steps": E},
+            "e2e": e2e,
             "diagnostics": {
                 "steps": args.warmup + K,
                 "energy_drift": _rel_change(diag1["total_energy"], diag0["total_energy"]),
@@ -687,7 +827,11 @@ def run_own(args):
     extras = world == 1
     if rank == 0 and extras:
         if not args.no_secondary and args.workload != "gaussian-mixture-16m":
-            out["secondary"] = secondary_16m(pkg, local)
+            out["secondary"] = secondary_16m(pkg, local, sm_max_mhz=clk.get("sm_max_mhz"),
+                                             hbm_gbs=out["hbm_peak_gbs"],
+                                             with_cpu=not args.no_cpu_baseline)
+        if not args.no_exact_walk and args.workload == "colliding-disks-800k":
+            out["exact_walk"] = exact_walk_cost(pkg, local)
         if not args.no_adjoint:
             out["adjoint"] = adjoint_cost(pkg, local)
         if not args.no_ensemble:

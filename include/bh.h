@@ -320,9 +320,13 @@ int bh_get_system_offsets(bh_sim* sim, uint32_t* offsets); /* num_systems + 1 en
  * Limit: n <= 262144 (larger n returns BH_ERR_INVALID_ARGUMENT).  Enqueued on
  * `stream` (a cudaStream_t, NULL = legacy default stream); calls no cudaMalloc
  * or cudaFree.  All calls share the static scratch: calls that overlap on the
- * GPU race, so serialise them.  The first call on a device looks the scratch
- * up with cudaGetSymbolAddress; make it before any stream capture.  Errors are
- * reported through bh_global_last_error(). */
+ * GPU race, so serialise them.  Every call looks the scratch up with
+ * cudaGetSymbolAddress in the current context.  Under CUDA's lazy module
+ * loading the first call on a device may load this library's module, which
+ * reserves the static array (about 11.5 MB) and may synchronise: a caller
+ * that must not allocate while running makes one warm-up call at start-up,
+ * before any stream capture.  Errors are reported through
+ * bh_global_last_error(). */
 int bh_build_hierarchy_static(const void* sorted_codes, int32_t morton_bits,
                               const uint32_t* sorted_ids, const float* mass, const float* pos,
                               uint32_t n, float* node4, uint32_t* node_children,
@@ -350,6 +354,15 @@ typedef struct bh_diagnostics {
 } bh_diagnostics;
 
 int bh_diagnostics_compute(bh_sim* sim, int with_potential, bh_diagnostics* out);
+
+/* FP64 direct-sum accelerations of sampled bodies (extension; the reference
+ * has no force check).  For each body index sample[k] (original order, host
+ * array, count <= 2^20), acc_out[2k], acc_out[2k+1] (host) receive
+ *   G sum_{j != i} m_j (x_j - x_i) / (|x_j - x_i|^2 + eps_ij^2)^(3/2)
+ * summed in FP64 over every body at the handle's current positions, with the
+ * softening of the handle's force law.  The error of a force walk is measured
+ * against these.  O(count * n) work; synchronises the handle's stream. */
+int bh_direct_forces_fp64(bh_sim* sim, const uint32_t* sample, uint32_t count, double* acc_out);
 
 /* ---- density render (the reference's Renderer, src/renderer.ts:1-329) --- */
 /* A headless replacement of the two render passes of Renderer.getCommands()
@@ -403,6 +416,31 @@ int bh_renderer_get_targets(bh_renderer* r, float** density, uint8_t** image, ui
 int bh_renderer_read_density(bh_renderer* r, float* host);
 int bh_renderer_read_image(bh_renderer* r, uint8_t* host);
 const char* bh_renderer_last_error(bh_renderer* r);
+
+/* ---- test hooks of the device-side checks (extension) -------------------- */
+/* No counterpart in the reference, whose walk silently drops stack pushes
+ * (barnes_hut.wgsl:100-105) and whose sort has no bounded wait.  The engine's
+ * kernels check themselves instead of hanging or writing out of bounds: the
+ * sort's decoupled look-back gives up after a bounded number of spins, and
+ * the walks refuse a push that would overflow their stack.  A tripped check
+ * sets the handle's device error word; the next synchronising call (bh_sync,
+ * bh_download, bh_compute_accelerations, ...) returns BH_ERR_DEVICE_CHECK
+ * with a message naming the check and clears the word.  After a failed sort
+ * the step's hierarchy build and walk skip their work, so a failed step
+ * leaves the bodies as they were before it (leapfrog: after its opening
+ * kick-drift).
+ * This call lowers those limits so a test can make them run out without
+ * faulting or hanging the GPU:
+ *   lookback_spin_cap  spins before the look-back gives up (0 = default,
+ *                      about 4M spins, several seconds)
+ *   walk_stack_cap     stack entries a walk warp may use (0 = full; >= 2)
+ *   flags              BH_DEBUG_LOOKBACK_UNPUBLISHED: the second tile of the
+ *                      first sort pass waits on a predecessor status that
+ *                      never reads as published (needs n > 6144 bodies)
+ * Zeros restore normal operation.  Takes effect from the next call. */
+#define BH_DEBUG_LOOKBACK_UNPUBLISHED 1u
+int bh_debug_set_limits(bh_sim* sim, uint32_t flags, uint32_t lookback_spin_cap,
+                        uint32_t walk_stack_cap);
 
 /* ---- errors ------------------------------------------------------------- */
 const char* bh_last_error(bh_sim* sim);

@@ -20,7 +20,10 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libbh_oracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
-REFERENCE_CHECKOUT = "/root/reference"
+# Where the reference checkout lies: BH_REFERENCE_CHECKOUT, or the build
+# container's mount point.  Absent (e.g. on a GPU host), oracle/_ref is not
+# rebuilt and the prebuilt files are used as they are.
+REFERENCE_CHECKOUT = os.environ.get("BH_REFERENCE_CHECKOUT") or "/root/reference"
 
 CFLAGS = ["-O3", "-march=x86-64-v2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math",
           "-fPIC", "-shared", "-std=c11", "-Wall"]

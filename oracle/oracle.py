@@ -359,6 +359,10 @@ def _ref_lib():
                                 ctypes.c_int] + [_P] * 11
         lib.ref_max_threads.restype = ctypes.c_int
         lib.ref_max_threads.argtypes = []
+        lib.ref_run_timed.restype = ctypes.c_int
+        lib.ref_run_timed.argtypes = [ctypes.c_uint32, _P, _P, _P, ctypes.c_float, ctypes.c_float,
+                                      ctypes.c_float, ctypes.c_float, ctypes.c_uint32,
+                                      ctypes.c_uint32, ctypes.c_int, _P]
         _ref = lib
     return _ref
 
@@ -391,6 +395,25 @@ def ref_run(mass, pos, vel, G=1.0, dt=0.1 / 60.0, eps_mult=1.0, theta=0.6, offse
                  _p(out["right"]), _p(out["parent"]), _p(out["com"]), _p(out["mass"]),
                  _p(out["aabb"]), _p(out["length"]))
     return out
+
+
+REF_STAGES = ("morton", "sort", "build_fill", "vel_step", "pos_step")
+
+
+def ref_run_timed(mass, pos, vel, G=1.0, dt=0.1 / 60.0, eps_mult=1.0, theta=0.6, steps=1,
+                  walk_stride=1, parallel=True) -> dict:
+    """Wall time per stage of `steps` steps of the translated reference
+    pipeline on all host threads; the velocity step (the walk) runs for every
+    `walk_stride`-th sorted slot only, so its time is a sample to be scaled
+    by walk_stride."""
+    _ref_lib()
+    mass = f32(mass)
+    out = np.zeros(5, np.float64)
+    rc = _ref.ref_run_timed(mass.size, _p(mass), _p(f32(pos, (-1, 2))), _p(f32(vel, (-1, 2))), G,
+                            dt, eps_mult, theta, steps, walk_stride, 1 if parallel else 0, _p(out))
+    if rc != 0:
+        raise ValueError("ref_run_timed: bad arguments")
+    return dict(zip(REF_STAGES, out.tolist()))
 
 
 class State:

@@ -1,0 +1,68 @@
+"""CPU checks of bench.py: the reference arm imports nothing of the engine,
+and its plain workload table agrees with the package's WORKLOADS."""
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _bench():
+    sys.path.insert(0, ROOT)
+    import importlib
+    return importlib.import_module("bench")
+
+
+def test_reference_workloads_match_the_package(bh):
+    bench = _bench()
+    for name, wp in bench.REF_WORKLOADS.items():
+        wl = bh.WORKLOADS[name]
+        assert wp["n"] == wl["n"] and wp["scenario"] == wl["scenario"], name
+        cfg = wl["config"]
+        op = wp["oracle"]
+        got = (op["G"], op["dt"], op["theta"], op["softening"], op["plummer_eps"],
+               op["morton_bits"], op["morton_domain"], op["integrator"], op["walk"],
+               op["multipole"])
+        want = (cfg.gravConstant, cfg.deltaTime, cfg.bhTheta, cfg.softening, cfg.plummerEps,
+                cfg.mortonBits, cfg.mortonDomain, cfg.integrator, cfg.walk, cfg.multipole)
+        assert got == want, name
+
+
+def test_reference_arm_runs_without_the_engine(orc):
+    # The reference arm on the small parity workload, in a fresh process:
+    # it prints its line and never maps the engine's library.
+    code = (
+        "import sys, json, runpy\n"
+        f"sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'uniform-disk-16k',"
+        " '--steps', '3', '--warmup', '3']\n"
+        "try:\n"
+        "    runpy.run_path('bench.py', run_name='__main__')\n"
+        "except SystemExit:\n"
+        "    pass\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('ENGINE_MAPPED' if 'libbh_b200' in maps else 'ENGINE_NOT_MAPPED')\n"
+        "print('PKG_IMPORTED' if 'webgpu-fluid-sim_b200' in sys.modules else 'PKG_NOT_IMPORTED')\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "ENGINE_NOT_MAPPED" in r.stdout and "PKG_NOT_IMPORTED" in r.stdout, r.stdout[-2000:]
+    import json
+    line = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][0])
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
+    assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_walk_roofline_flop_convention():
+    bench = _bench()
+
+    class C:
+        walk, multipole = "group", 2
+
+    r = bench.walk_roofline(C, 1.0, 1000, 100, 10, 1965.0)
+    assert r["flops_per_step"] == 35 * 1000 + 16 * 100
+    assert r["achieved"] == pytest.approx(r["flops_per_step"] / 1e-3 / 1e12)
+    s = bench.stream_rooflines({"sort": 1.0}, 1_000_000, 8, 6000.0)
+    assert s["sort"]["bytes_per_body"] == 20 + 7 * 24

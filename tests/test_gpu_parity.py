@@ -179,6 +179,54 @@ def test_split_build_matches_oracle_beyond_2m(bh, orc, cfg):
     sim.close()
 
 
+def test_headline_workload_tree_matches_oracle_800k(bh, orc):
+    # The benchmark workload itself (800,000 bodies, two colliding disks,
+    # 32-bit keys over the bounding box, group-walk records): every tree
+    # array bit for bit against the oracle, node values within tolerance,
+    # and the force error against the FP64 direct sum on 2,048 bodies.
+    wl = bh.WORKLOADS["colliding-disks-800k"]
+    n = wl["n"]
+    sim = bh.Simulation(wl["config"])
+    sim.setNumBodies(n)
+    sim.setScenario(wl["scenario"], 1)
+    mass, pos, vel = sim.download()
+    acc = sim.computeAccelerations()
+    t = sim.tree()
+    p = orc.params_from_config(sim.config)
+    codes, ids = orc.morton(p, pos)
+    codes, ids = orc.sort(codes, ids)
+    left, right, parent = orc.build(codes, sim.config.mortonBits)
+    com, mnode, aabb, length = orc.fill(ids, mass, pos, left, right, parent)
+    assert (t["codes"].astype(np.uint64) == codes).all(), "Morton codes differ"
+    assert (t["ids"] == ids).all(), "sorted permutation differs"
+    assert (t["parent"] == parent).all(), "parent array differs"
+    assert (t["children"][:, 0] == left[: n - 1]).all(), "left children differ"
+    assert (t["children"][:, 1] == right[: n - 1]).all(), "right children differ"
+    assert (t["aabb"] == aabb[: n - 1]).all(), "AABBs differ"
+    assert (t["node4"][:, 3] == length).all(), "lengths differ"
+    assert np.all(np.abs(t["node4"][:, 2] - mnode) <= 1e-5 * np.abs(mnode) + 1e-30)
+    scale = np.abs(com).max(1) + length
+    assert np.all(np.abs(t["node4"][:, :2] - com).max(1) <= 1e-5 * scale + 1e-30)
+    fe = sim.forceError(acc, nsample=2048, seed=5)
+    print(f"800k group walk: FP64 error median {fe['median']:.3e} p99 {fe['p99']:.3e}")
+    assert fe["median"] <= 1e-3
+    sim.close()
+
+
+def test_direct_forces_fp64_matches_oracle(bh, orc):
+    # The GPU FP64 direct sum used to measure every force error, against the
+    # oracle's FP64 direct sum (both softening laws).
+    for cfg in (dict(GROUP), dict(bhTheta=0.5)):
+        sim = make_sim(bh, 30000, "colliding-disks" if "walk" in cfg else "default", seed=2, **cfg)
+        mass, pos, _ = sim.download()
+        sample = np.sort(np.random.default_rng(3).choice(30000, 500, replace=False))
+        got = sim.directForcesFp64(sample)
+        ref = orc.direct_sum_fp64(orc.params_from_config(sim.config), mass, pos, sample)
+        rel = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        assert rel.max() <= 1e-7, rel.max()  # FP32 sums would miss by ~1e-5
+        sim.close()
+
+
 def test_graph_and_direct_paths_agree(bh):
     outs = []
     for graphs in (True, False):

@@ -23,14 +23,23 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
-@pytest.mark.parametrize("cfg", [
-    dict(mortonDomain="bbox", softening="plummer", bhTheta=0.5),
-    dict(mortonBits=64, softening="plummer", bhTheta=0.5),
-])
-def test_static_build_matches_engine_on_two_calls(bh, cfg):
+def _free_device_bytes():
+    import torch
+    torch.cuda.synchronize()
+    return torch.cuda.mem_get_info()[0]
+
+
+@pytest.mark.parametrize("n,cfg", [
+    (120_000, dict(mortonDomain="bbox", softening="plummer", bhTheta=0.5)),
+    (120_000, dict(mortonBits=64, softening="plummer", bhTheta=0.5)),
+    (STATIC_MAX, dict(mortonDomain="bbox", softening="plummer", bhTheta=0.5)),  # the whole array
+    (STATIC_MAX, dict(mortonBits=64, softening="plummer", bhTheta=0.5)),
+    (1, dict(mortonDomain="bbox", softening="plummer", bhTheta=0.5)),  # a lone leaf
+    (2, dict(mortonDomain="bbox", softening="plummer", bhTheta=0.5)),  # the smallest tree
+], ids=["120k-32bit", "120k-64bit", "limit-32bit", "limit-64bit", "n1", "n2"])
+def test_static_build_matches_engine_on_two_calls(bh, n, cfg):
     import torch
     lib = bh.load()
-    n = 120_000
     sim = bh.Simulation(bh.Config(**cfg))
     sim.setNumBodies(n)
     sim.setScenario("colliding-disks", 5)
@@ -39,24 +48,30 @@ def test_static_build_matches_engine_on_two_calls(bh, cfg):
     b = sim.getBuffers()
     dev = torch.device("cuda", 0)
     node4 = torch.empty(4 * (2 * n - 1), dtype=torch.float32, device=dev)
-    children = torch.empty(2 * (n - 1), dtype=torch.int32, device=dev)
+    # n == 1 has no internal node: the entry point takes null children / boxes
+    children = torch.empty(max(2 * (n - 1), 1), dtype=torch.int32, device=dev)
     parent = torch.empty(2 * n - 1, dtype=torch.int32, device=dev)
-    aabb = torch.empty(4 * (n - 1), dtype=torch.float32, device=dev)
+    aabb = torch.empty(max(4 * (n - 1), 1), dtype=torch.float32, device=dev)
     bits = sim.config.mortonBits
     for call in range(2):
         for t in (node4, children, parent, aabb):
             t.fill_(-7)  # stale contents must all be overwritten
-        torch.cuda.synchronize()
+        free_before = _free_device_bytes()
         rc = lib.bh_build_hierarchy_static(
             ctypes.c_void_p(b.mortonCodes), bits, ctypes.c_void_p(b.bodyIndices),
-            ctypes.c_void_p(b.mass), ctypes.c_void_p(b.pos), n, _ptr(node4), _ptr(children),
-            _ptr(parent), _ptr(aabb), 1, ctypes.c_void_p(b.stream))
+            ctypes.c_void_p(b.mass), ctypes.c_void_p(b.pos), n, _ptr(node4),
+            _ptr(children) if n > 1 else None, _ptr(parent), _ptr(aabb) if n > 1 else None, 1,
+            ctypes.c_void_p(b.stream))
         assert rc == 0, lib.bh_global_last_error()
         sim.sync()  # enqueued on the engine's stream
+        if call == 1:
+            # After the first call (which may load the module holding the
+            # static array), a call changes no device allocation.
+            assert _free_device_bytes() == free_before, "the entry point allocated device memory"
         got4 = node4.cpu().numpy().reshape(-1, 4)
-        got_children = children.cpu().numpy().view(np.uint32).reshape(-1, 2)
+        got_children = children.cpu().numpy().view(np.uint32)[: 2 * (n - 1)].reshape(-1, 2)
         got_parent = parent.cpu().numpy().view(np.uint32)
-        got_aabb = aabb.cpu().numpy().reshape(-1, 4)
+        got_aabb = aabb.cpu().numpy()[: 4 * (n - 1)].reshape(-1, 4)
         assert np.array_equal(got_children, ref["children"]), f"call {call}: children differ"
         assert np.array_equal(got_parent, ref["parent"]), f"call {call}: parents differ"
         assert np.array_equal(got_aabb, ref["aabb"]), f"call {call}: boxes differ"

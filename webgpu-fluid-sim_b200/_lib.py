@@ -29,6 +29,8 @@ BH_INTEGRATOR_LEAPFROG_KDK = 1
 
 BH_STAGE_NAMES = ("morton", "sort", "tree", "walk", "other")
 
+BH_DEBUG_LOOKBACK_UNPUBLISHED = 1
+
 
 class bh_config(ctypes.Structure):
     _fields_ = [
@@ -146,6 +148,8 @@ SIGNATURES = {
     "bh_shard_pack": (ctypes.c_int, [_P, _P, ctypes.c_uint32]),
     "bh_shard_unpack": (ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint32]),
     "bh_diagnostics_compute": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(bh_diagnostics)]),
+    "bh_direct_forces_fp64": (ctypes.c_int, [_P, _P, ctypes.c_uint32, _P]),
+    "bh_debug_set_limits": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
     "bh_renderer_create": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_P)]),
     "bh_renderer_destroy": (ctypes.c_int, [_P]),
     "bh_renderer_resize": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32]),

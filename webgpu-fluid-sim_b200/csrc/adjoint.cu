@@ -104,6 +104,7 @@ vjp_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ nod
                  float2* __restrict__ xbar_slot, float* __restrict__ mbar_slot,
                  const WalkParams P, uint32_t* __restrict__ err) {
     __shared__ VjpSmem smem[kVjpWarps];
+    if (step_failed(err)) return;  // the tree at these positions was not built
     const int lane = threadIdx.x & 31;
     VjpSmem& S = smem[threadIdx.x >> 5];
     const unsigned FULL = 0xFFFFFFFFu;

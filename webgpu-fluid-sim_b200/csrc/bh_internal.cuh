@@ -34,6 +34,14 @@ constexpr int kRadix = 256;
 constexpr uint32_t kErrLookbackSpin = 1u << 0;  // decoupled look-back gave up waiting
 constexpr uint32_t kErrStackOverflow = 1u << 1; // walk stack would have overflowed (children dropped)
 constexpr uint32_t kErrTreeSpin = 1u << 2;
+// Failures after which the rest of a step has no valid input: the build and
+// the walk then skip their work for that step instead of consuming it.
+constexpr uint32_t kErrSkipMask = kErrLookbackSpin;
+// Default spins of the sort's bounded look-back wait (several seconds).
+constexpr uint32_t kSpinCapDefault = 1u << 22;
+// Test hook: the second tile of the first sort pass waits on a predecessor
+// status that never reads as published, so its bounded wait runs out.
+constexpr uint32_t kDebugLookbackUnpublished = 1u << 0;
 
 // Packed internal-node record of the group walk (64 B, one per internal node):
 // the criterion reads `box`, an accepted node contributes `mom` + `quad`, an
@@ -60,6 +68,12 @@ __device__ __forceinline__ bool group_accepts(const float4& box, float cx, float
     const float sx = fmaxf(__fsub_rn(box.x, ghix), __fsub_rn(glox, box.z));
     const float sy = fmaxf(__fsub_rn(box.y, ghiy), __fsub_rn(gloy, box.w));
     return __fmul_rn(L, L) < __fmul_rn(th2, d2) && (sx > 0.0f || sy > 0.0f);
+}
+
+// True when an earlier stage of this step left no valid input (its bounded
+// wait gave up, kErrSkipMask); the build and the walk then skip their work.
+__device__ __forceinline__ bool step_failed(const uint32_t* err) {
+    return err && (__ldcg(err) & kErrSkipMask) != 0u;
 }
 
 // Reciprocal square root with subnormal inputs flushed to zero, which drops
@@ -109,6 +123,9 @@ struct WalkParams {
     // sharding: only groups whose first sorted slot lies in [slot_lo, slot_hi)
     uint32_t slot_lo;
     uint32_t slot_hi;
+    // stack entries a warp may use (0 = the kernel's full capacity); a test
+    // lowers it to make the overflow check trip
+    int stack_cap = 0;
 };
 
 // Per-step scratch that must start at zero.  One memset clears it.
@@ -155,6 +172,8 @@ struct DeviceBuffers {
     uint32_t* status = nullptr;  // look-back status: passes * tiles * 256
     uint32_t tiles = 0;
     uint32_t* err = nullptr;     // device error word
+    uint32_t spin_cap = kSpinCapDefault;  // sort look-back wait bound (spins)
+    uint32_t debug_flags = 0;    // kDebug* test hooks
     int sort_passes = 0;         // 0: one per key byte; ensembles sort fewer (even count)
     // ensemble of independent systems (num_systems = 0: one system)
     uint32_t num_systems = 0;

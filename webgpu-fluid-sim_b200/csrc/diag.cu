@@ -117,6 +117,52 @@ potential_kernel(const float* __restrict__ mass, const float2* __restrict__ pos,
     }
 }
 
+// FP64 direct-sum acceleration of sampled bodies: block (k, c) adds body
+// sample[k]'s pull from the bodies of chunk c.  Consecutive blocks take
+// consecutive samples of the same chunk, so the blocks resident together
+// read the same ~1M bodies and the chunk is read from DRAM about once.
+constexpr uint32_t kDirectChunks = 16;
+
+__global__ void __launch_bounds__(kDiagThreads)
+direct_fp64_kernel(const float* __restrict__ mass, const float2* __restrict__ pos, uint32_t n,
+                   const uint32_t* __restrict__ sample, int plummer, double eps2, double eps_coef,
+                   double* __restrict__ out) {
+    __shared__ double s[2][kDiagThreads / 32];
+    const uint32_t i = sample[blockIdx.x];
+    const uint32_t chunk = (n + gridDim.y - 1) / gridDim.y;
+    const uint32_t lo = blockIdx.y * chunk;
+    const uint32_t hi = (lo + chunk) < n ? (lo + chunk) : n;
+    const float2 pi = pos[i];
+    const double xi = pi.x, yi = pi.y, mi = mass[i];
+    double ax = 0.0, ay = 0.0;
+    for (uint32_t j = lo + threadIdx.x; j < hi; j += kDiagThreads) {
+        if (j == i) continue;
+        const float2 pj = pos[j];
+        const double mj = mass[j];
+        const double dx = (double)pj.x - xi, dy = (double)pj.y - yi;
+        const double e2 = plummer ? eps2 : eps_coef * fmax(mi, mj);
+        const double r2 = dx * dx + dy * dy + e2;
+        if (!(r2 > 0.0)) continue;
+        const double inv = rsqrt(r2);
+        const double f = mj * inv * inv * inv;
+        ax += f * dx;
+        ay += f * dy;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    ax = warp_sum_d(ax);
+    ay = warp_sum_d(ay);
+    if (lane == 0) {
+        s[0][warp] = ax;
+        s[1][warp] = ay;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double t = 0.0;
+        for (int w = 0; w < kDiagThreads / 32; ++w) t += s[threadIdx.x][w];
+        atomicAdd(&out[2 * (size_t)blockIdx.x + threadIdx.x], t);
+    }
+}
+
 bool sim_body_view(const bh_sim* s, BodyView* out);
 void set_global_error(const std::string& msg);
 
@@ -173,5 +219,51 @@ extern "C" int bh_diagnostics_compute(bh_sim* sim, int with_potential, bh_diagno
     // each pair was summed from both sides
     out->potential_energy = with_potential ? -0.5 * (double)cfg.grav_constant * h[7] : NAN;
     out->pairs = (with_potential && v.n > 1) ? (uint64_t)v.n * (v.n - 1) / 2 : 0;
+    return BH_OK;
+}
+
+extern "C" int bh_direct_forces_fp64(bh_sim* sim, const uint32_t* sample, uint32_t count,
+                                     double* acc_out) {
+    if (!sim || (count && (!sample || !acc_out)))
+        return dfail(BH_ERR_INVALID_ARGUMENT, "bh_direct_forces_fp64: null argument");
+    if (count > (1u << 20))
+        return dfail(BH_ERR_INVALID_ARGUMENT, "bh_direct_forces_fp64: at most 2^20 samples per call");
+    bh_config cfg;
+    const int st = bh_get_config(sim, &cfg);
+    if (st != BH_OK) return st;
+    bh::BodyView v;
+    bh::sim_body_view(sim, &v);
+    for (uint32_t k = 0; k < count; ++k)
+        if (sample[k] >= v.n) return dfail(BH_ERR_INVALID_ARGUMENT, "bh_direct_forces_fp64: sample index out of range");
+    if (count == 0) return BH_OK;
+    cudaError_t e = cudaSetDevice(v.device);
+    if (e != cudaSuccess) return dfail(BH_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    const size_t out_bytes = 2 * sizeof(double) * (size_t)count;
+    const size_t idx_off = (out_bytes + 255) & ~(size_t)255;
+    unsigned char* d = nullptr;
+    e = cudaMallocAsync((void**)&d, idx_off + 4 * (size_t)count, v.stream);
+    if (e != cudaSuccess) return dfail(BH_ERR_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    double* dacc = reinterpret_cast<double*>(d);
+    uint32_t* didx = reinterpret_cast<uint32_t*>(d + idx_off);
+    e = cudaMemsetAsync(dacc, 0, out_bytes, v.stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(didx, sample, 4 * (size_t)count, cudaMemcpyHostToDevice, v.stream);
+    if (e == cudaSuccess) {
+        const int plummer = cfg.softening == BH_SOFTENING_PLUMMER;
+        const double eps2 = (double)cfg.plummer_eps * (double)cfg.plummer_eps;
+        // (epsMult sqrt(G dt m))^2, barnes_hut.wgsl:90-92
+        const double coef = (double)cfg.epsilon_multiplier * cfg.epsilon_multiplier *
+                            cfg.grav_constant * cfg.delta_time;
+        uint32_t chunks = bh::kDirectChunks;
+        if (v.n < chunks * bh::kDiagThreads) chunks = 1;
+        bh::direct_fp64_kernel<<<dim3(count, chunks), bh::kDiagThreads, 0, v.stream>>>(
+            v.mass, v.pos, v.n, didx, plummer, eps2, coef, dacc);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(acc_out, dacc, out_bytes, cudaMemcpyDeviceToHost, v.stream);
+    cudaFreeAsync(d, v.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(v.stream);
+    if (e != cudaSuccess) return dfail(BH_ERR_CUDA, std::string("direct forces: ") + cudaGetErrorString(e));
+    const double G = cfg.grav_constant;
+    for (size_t k = 0; k < 2 * (size_t)count; ++k) acc_out[k] *= G;
     return BH_OK;
 }

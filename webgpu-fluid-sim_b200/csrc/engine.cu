@@ -35,6 +35,8 @@ struct bh_sim {
     bool device_gen = false;  // the scenario comes from the GPU generators
     // sharding: the step's walk integrates only groups starting in these slots
     uint32_t shard_lo = 0, shard_hi = 0xFFFFFFFFu;
+    // test hooks of the device-side checks (bh_debug_set_limits): 0 = defaults
+    uint32_t debug_flags = 0, debug_spin_cap = 0, debug_stack_cap = 0;
     DeviceBuffers b;
     void* arena = nullptr;
     size_t arena_bytes = 0;
@@ -346,6 +348,8 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     b.status = (uint32_t*)(a + o_status);
     b.tiles = tiles;
     b.err = (uint32_t*)(a + o_err);
+    b.spin_cap = s->debug_spin_cap ? s->debug_spin_cap : bh::kSpinCapDefault;
+    b.debug_flags = s->debug_flags;
     BH_CUDA(s, cudaMemsetAsync(arena, 0, c.off, s->stream));
     BH_CUDA(s, cudaMemsetAsync(b.bound, 0xFF, sizeof(uint32_t) * ni, s->stream));
     if (E) {
@@ -406,6 +410,7 @@ static bh::WalkParams walk_params(const bh_sim* s, int mode) {
     const bool integrating = mode == bh::kWalkEulerKickDrift || mode == bh::kWalkKdkClose;
     p.slot_lo = integrating ? s->shard_lo : 0u;
     p.slot_hi = integrating ? s->shard_hi : 0xFFFFFFFFu;
+    p.stack_cap = (int)s->debug_stack_cap;
     return p;
 }
 
@@ -1228,6 +1233,24 @@ extern "C" int bh_walk_stats(bh_sim* s, uint64_t* node_visits, uint64_t* multipo
     if (multipole_interactions) *multipole_interactions = h[1];
     if (body_interactions) *body_interactions = h[2];
     return check_device_errors(s);
+}
+
+// ---- test hooks of the device-side checks ------------------------------------------
+
+extern "C" int bh_debug_set_limits(bh_sim* s, uint32_t flags, uint32_t lookback_spin_cap,
+                                   uint32_t walk_stack_cap) {
+    BH_HANDLE(s);
+    if (flags & ~bh::kDebugLookbackUnpublished)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_debug_set_limits: unknown flag");
+    if (walk_stack_cap == 1)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_debug_set_limits: a walk stack needs 2 entries");
+    s->debug_flags = flags;
+    s->debug_spin_cap = lookback_spin_cap;
+    s->debug_stack_cap = walk_stack_cap;
+    s->b.spin_cap = lookback_spin_cap ? lookback_spin_cap : bh::kSpinCapDefault;
+    s->b.debug_flags = flags;
+    destroy_graphs(s);  // captured steps carry the old kernel parameters
+    return BH_OK;
 }
 
 // ---- buffers -----------------------------------------------------------------------

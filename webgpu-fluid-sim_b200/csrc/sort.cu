@@ -33,7 +33,6 @@ constexpr uint32_t kFlagAggregate = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kFlagMask = 3u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1;
-constexpr uint32_t kSpinCap = 1u << 22;
 #ifndef BH_SORT_LOOK_BATCH
 #define BH_SORT_LOOK_BATCH 4
 #endif
@@ -68,7 +67,7 @@ __global__ void __launch_bounds__(kSortThreads, BH_SORT_MIN_BLOCKS)
 onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_in,
                 K* __restrict__ keys_out, uint32_t* __restrict__ ids_out, uint32_t n, int pass,
                 StepScratch* __restrict__ scratch, uint32_t* __restrict__ status, uint32_t tiles,
-                uint32_t* __restrict__ err) {
+                uint32_t* __restrict__ err, uint32_t spin_cap, uint32_t debug_flags) {
     constexpr int W = kSortThreads / 32;
     __shared__ uint32_t s_whist[W][kRadix];
     __shared__ uint32_t s_tile_excl[kRadix];
@@ -186,6 +185,9 @@ onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_
                     v[j] = a.load(cuda::memory_order_relaxed);
                 }
             }
+            // Test hook: tile 1 of the first pass never sees its only
+            // predecessor, tile 0 (entry j = 0), publish.
+            if (FIRST && (debug_flags & kDebugLookbackUnpublished) && tile == 1u) v[0] = 0u;
             bool done = false;
             int used = 0;
 #pragma unroll
@@ -198,7 +200,7 @@ onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_
             if (done) break;
             t -= used;
             if (used == 0) {
-                if (++spins > kSpinCap) {
+                if (++spins > spin_cap) {
                     atomicOr(err, kErrLookbackSpin);
                     break;
                 }
@@ -241,10 +243,12 @@ static void sort_impl(const DeviceBuffers& b, cudaStream_t s) {
     for (int p = 0; p < passes; ++p) {
         if (p == 0)
             onesweep_kernel<K, true><<<b.tiles, kSortThreads, smem, s>>>(
-                kin, nullptr, kout, iout, b.n, p, b.scratch, b.status, b.tiles, b.err);
+                kin, nullptr, kout, iout, b.n, p, b.scratch, b.status, b.tiles, b.err, b.spin_cap,
+                b.debug_flags);
         else
             onesweep_kernel<K, false><<<b.tiles, kSortThreads, smem, s>>>(
-                kin, iin, kout, iout, b.n, p, b.scratch, b.status, b.tiles, b.err);
+                kin, iin, kout, iout, b.n, p, b.scratch, b.status, b.tiles, b.err, b.spin_cap,
+                b.debug_flags);
         K* tk = kin; kin = kout; kout = tk;
         uint32_t* ti = iin; iin = iout; iout = ti;
     }

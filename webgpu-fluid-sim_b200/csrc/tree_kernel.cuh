@@ -97,6 +97,9 @@ struct BuildArgs {
     // {x, y, m, 0} per body in original order, when the encode wrote them:
     // one gather per slot instead of a position and a mass
     const float4* xm = nullptr;
+    // The step's device error word: when an earlier stage of the step failed
+    // (kErrSkipMask), the build does nothing.  Null: no such check.
+    const uint32_t* err = nullptr;
 };
 
 // One thread per sorted slot climbs from its leaf; the lanes of a warp start
@@ -373,6 +376,7 @@ build_fill_kernel(const BuildArgs<K> A) {
     __shared__ BuildShared<K, B> S;
 
     const uint32_t n = A.n;
+    if (step_failed(A.err)) return;  // uniform over the block
     const int t = (int)threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint32_t B0 = blockIdx.x * (uint32_t)B;
     const uint32_t i = B0 + (uint32_t)t;
@@ -476,6 +480,7 @@ build_fill_kernel(const BuildArgs<K> A) {
 template <typename K>
 __global__ void __launch_bounds__(kClimbBlock)
 build_climb_kernel(const BuildArgs<K> A) {
+    if (step_failed(A.err)) return;
     const uint32_t count = *A.frontier_count;
     const uint32_t n = A.n, nm1 = n - 1;
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {

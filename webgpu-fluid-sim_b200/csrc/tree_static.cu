@@ -18,12 +18,14 @@
 //    other parts are written before they are read.  Calls whose kernels
 //    overlap on the GPU (different streams, or different host threads on
 //    the same device) race on the array: serialise them;
-//  - the first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress (once per device, that device current); make that
-//    first call before any stream capture.
+//  - every call looks up the array's device address on the current device
+//    with cudaGetSymbolAddress (no cached pointer outlives a context reset);
+//    under CUDA's lazy module loading the first call on a device may load
+//    the library's module, which reserves the array and may synchronise, so
+//    a caller that must not allocate while running makes one warm-up call
+//    at start-up, and before any stream capture.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "bh.h"
@@ -44,24 +46,14 @@ constexpr size_t kScratchBytes = align_up(kBigOff + 2 * sizeof(double2) * (kStat
 
 static __device__ __align__(256) unsigned char g_tree_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-static std::mutex g_setup_mutex;
-static unsigned char* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of g_tree_scratch on the current device (looked up once).
+// Device address of g_tree_scratch in the current context.  Looked up on
+// every call: cheap once the module is loaded, and never stale after a
+// cudaDeviceReset or a new primary context.
 static cudaError_t scratch_address(unsigned char** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_tree_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_tree_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_addr[dev] = static_cast<unsigned char*>(p);
-    }
-    *out = g_scratch_addr[dev];
+    *out = static_cast<unsigned char*>(p);
     return cudaSuccess;
 }
 

@@ -35,6 +35,8 @@ walk_kernel(const float4* __restrict__ node4, const uint2* __restrict__ children
             const WalkParams P, uint32_t* __restrict__ err) {
     constexpr int kWarps = 256 / 32;
     __shared__ uint2 s_stack[kWarps][kStackSize];
+    if (step_failed(err)) return;  // the tree of this step was not built
+    const int stack_cap = (P.stack_cap > 0 && P.stack_cap < kStackSize) ? P.stack_cap : kStackSize;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n = P.n, nm1 = n - 1;
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -94,7 +96,7 @@ walk_kernel(const float4* __restrict__ node4, const uint2* __restrict__ children
                     continue;
                 }
             }
-            if (sp < kStackSize - 1) {  // barnes_hut.wgsl:100: stack_ptr + 2 < stack_size
+            if (sp < stack_cap - 1) {  // barnes_hut.wgsl:100: stack_ptr + 2 < stack_size
                 const uint2 ch = __ldg(&children[node]);
                 if (lane == 0) {
                     stk[sp] = make_uint2(ch.x, open);

@@ -77,6 +77,7 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
                   const WalkParams P, uint32_t* __restrict__ err) {
     constexpr int NP = BPL / 2;  // packed pairs per lane (BPL >= 2)
     __shared__ GroupSmem smem[kGroupWarps];
+    if (step_failed(err)) return;  // the tree of this step was not built
     const int lane = threadIdx.x & 31;
     GroupSmem& S = smem[threadIdx.x >> 5];
     const unsigned FULL = 0xFFFFFFFFu;
@@ -89,6 +90,7 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
     const bool self_test = !(PLUMMER && eps2 > 0.0f);
     const bool counting = P.count != 0;
     unsigned long long c_vis = 0, c_node = 0, c_body = 0;
+    const int stack_cap = (P.stack_cap > 0 && P.stack_cap < kWalkStack) ? P.stack_cap : kWalkStack;
 
     while (true) {
         uint32_t g = 0;
@@ -333,7 +335,7 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
             }
             const unsigned mp = __ballot_sync(FULL, push);
             const int npush = 2 * __popc(mp);
-            if (sp + npush <= kWalkStack) {
+            if (sp + npush <= stack_cap) {
                 if (push) {
                     const int p = sp + 2 * __popc(mp & lt);
                     S.stack[p] = r1;      // right child

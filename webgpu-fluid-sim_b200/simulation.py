@@ -275,6 +275,35 @@ class Simulation:
             out["pairs"] = int(d.pairs)
         return out
 
+    def directForcesFp64(self, sample) -> np.ndarray:
+        """FP64 direct-sum accelerations (G included) of the bodies whose
+        original indices are in ``sample``, at the current positions."""
+        idx = np.ascontiguousarray(sample, dtype=np.uint32).reshape(-1)
+        out = np.empty((idx.size, 2), np.float64)
+        self._check(self._lib.bh_direct_forces_fp64(self._h, _ptr(idx), int(idx.size), _ptr(out)))
+        return out
+
+    def forceError(self, acc, nsample: int = 1024, seed: int = 0) -> dict:
+        """Relative error |acc_i - a_i| / |a_i| of walk accelerations ``acc``
+        (original order) against the FP64 direct sum, on ``nsample`` bodies
+        drawn without replacement: median, p99, max and the sample size."""
+        n = self.getNumBodies()
+        rng = np.random.default_rng(seed)
+        idx = np.sort(rng.choice(n, size=min(nsample, n), replace=False)).astype(np.uint32)
+        ref = self.directForcesFp64(idx)
+        a = np.asarray(acc, dtype=np.float64).reshape(n, 2)[idx]
+        den = np.maximum(np.linalg.norm(ref, axis=1), 1e-300)
+        err = np.linalg.norm(a - ref, axis=1) / den
+        return {"median": float(np.median(err)), "p99": float(np.percentile(err, 99)),
+                "max": float(err.max()), "sample": int(idx.size)}
+
+    def debugSetLimits(self, flags: int = 0, lookback_spin_cap: int = 0,
+                       walk_stack_cap: int = 0) -> None:
+        """Test hook (bh_debug_set_limits): lower the bounded waits and stack
+        capacities of the device-side checks; zeros restore the defaults."""
+        self._check(self._lib.bh_debug_set_limits(self._h, int(flags), int(lookback_spin_cap),
+                                                  int(walk_stack_cap)))
+
     def kernels_per_step(self) -> int:
         k = ctypes.c_uint32()
         self._check(self._lib.bh_kernels_per_step(self._h, ctypes.byref(k)))
