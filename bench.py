@@ -149,16 +149,26 @@ def adjoint_cost(pkg, device: int, n: int = 65536, steps: int = 200, every: int 
             "timing": "host wall clock around synchronised calls, best of 3"}
 
 
+FAR_PAIR_FLOPS = 435.0  # one node's local coefficients (far_field.cuh, counted from the code)
+FAR_BODY_FLOPS = 50.0   # one body's local-expansion evaluation
+
+
 def walk_roofline(cfg, walk_ms: float, multi_inter: int, body_inter: int, visits: int,
-                  sm_max_mhz, traffic=None) -> dict:
+                  sm_max_mhz, traffic=None, far_pairs: int = 0, n: int = 0) -> dict:
     """Roofline of the walk: algorithmic FP32 flops per launch over its time,
     against the nominal FP32 FMA rate.  Flops: 16 per monopole interaction
     (2 sub, 3 for d^2+eps^2, 4 for rsqrt, 2 for inv^3, 1 for m inv^3, 4 for
     two FMA) and 35 per monopole + quadrupole interaction (the 16 plus Q'r 6,
     r.Q'r 3, inv^5 1, 2.5 r.Q'r inv^7 3, two extra FMA 4, one add 2), times
-    the interactions an instrumented launch of the same walk counts."""
+    the interactions an instrumented launch of the same walk counts; with the
+    far field, 435 per (far node, group) pair (local coefficients of orders
+    1-4: 79 polynomial terms of kernel derivatives up to order 6 at 3 flops,
+    14 coefficients at 12, set-up 30) and 50 per body for the expansion's
+    evaluation."""
     quad = cfg.walk == "group" and cfg.multipole >= 2
     flops = (35.0 if quad else 16.0) * multi_inter + 16.0 * body_inter
+    if far_pairs:
+        flops += FAR_PAIR_FLOPS * far_pairs + FAR_BODY_FLOPS * n
     mhz = sm_max_mhz or 1965.0
     fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12  # nominal FMA peak at max clock
     achieved = flops / (walk_ms / 1e3) / 1e12
@@ -170,6 +180,7 @@ def walk_roofline(cfg, walk_ms: float, multi_inter: int, body_inter: int, visits
             "kernel": "walk", "kernel_ms": walk_ms,
             "multipole_interactions_per_step": multi_inter,
             "body_interactions_per_step": body_inter,
+            "far_node_group_pairs_per_step": far_pairs,
             "node_visits_per_step": visits, "flops_per_step": flops}
 
 
@@ -248,7 +259,7 @@ def secondary_16m(pkg, device: int, steps: int = 5, e2e_steps: int = 3, sm_max_m
     ms = e0.elapsed_time(e1) / steps
     stages = {k: v / max(rec, 1) for k, v in stage_ms.items()}
     cfg = sim.config
-    visits, multi, body = sim.walk_stats()
+    visits, multi, body, far = sim.walk_stats()
     acc = sim.read_buffer("acc", np.float32, 2 * n).reshape(n, 2)
     ferr = sim.forceError(acc, nsample=1024, seed=1)
     e2e = e2e_rate(sim, sim.step, n, e2e_steps, ext)
@@ -257,7 +268,8 @@ def secondary_16m(pkg, device: int, steps: int = 5, e2e_steps: int = 3, sm_max_m
     out = {"workload": "gaussian-mixture-16m", "bodies": n, "metric": "body-steps/s",
            "value": n / (ms / 1e3), "unit": "body-steps/s", "ms_per_step": ms, "steps": steps,
            "stages_ms": stages,
-           "roofline": walk_roofline(cfg, stages["walk"], multi, body, visits, sm_max_mhz),
+           "roofline": walk_roofline(cfg, stages["walk"], multi, body, visits, sm_max_mhz,
+                                     far_pairs=far, n=n),
            "stream_stages": stream_rooflines(stages, n, 8, hbm_gbs),
            "force_error_vs_fp64": ferr, "e2e": e2e, "autotune": tune,
            "gpu_launches": kps * steps,
@@ -759,7 +771,7 @@ def run_own(args):
     diag1 = sim.diagnostics() if rank == 0 else None
 
     # ---- walk statistics + force error (untimed) ----
-    visits, multi_inter, body_inter = sim.walk_stats()
+    visits, multi_inter, body_inter, far_pairs = sim.walk_stats()
     acc = sim.read_buffer("acc", np.float32, 2 * n).reshape(n, 2)
     ferr = sim.forceError(acc, nsample=2048, seed=0) if rank == 0 else None
 
@@ -776,7 +788,8 @@ def run_own(args):
         # dominant kernel: the walk
         stages = {k: v / max(recorded, 1) for k, v in stage_ms.items()}
         roofline = walk_roofline(cfg, stages["walk"], multi_inter, body_inter, visits,
-                                 clk.get("sm_max_mhz"), NCU_WALK_TRAFFIC_BYTES.get(args.workload))
+                                 clk.get("sm_max_mhz"), NCU_WALK_TRAFFIC_BYTES.get(args.workload),
+                                 far_pairs=far_pairs, n=n)
         hbm = peaks.get("hbm_gbs", 6650.0)
         kps = sim.kernels_per_step()
         cb = None

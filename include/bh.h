@@ -71,7 +71,11 @@ typedef struct bh_config {
     int32_t walk_mode;        /* BH_WALK_EXACT (reference per-body walk) or BH_WALK_GROUP */
     int32_t multipole_order;  /* group walk: 1 = monopole, 2 = monopole + quadrupole */
     int32_t bodies_per_lane;  /* group walk: 1, 2 or 4 (group = 32 x this many bodies); 0 = 2 */
-    int32_t reserved[4];
+    float far_alpha;          /* group walk, Plummer softening: an accepted node whose distance R
+                                 from the group's box centre exceeds r_g / far_alpha (r_g = the
+                                 box's half-diagonal) acts through one local expansion per group
+                                 instead of on each body (0 = off; at most 0.5) */
+    int32_t reserved[3];
 } bh_config;
 
 #define BH_WALK_EXACT 0 /* lane-exact replica of barnes_hut.wgsl:48-111 (monopole, per-body theta test) */
@@ -235,10 +239,12 @@ int bh_kernels_per_step(bh_sim* sim, uint32_t* out);
 /* Build the tree at the current positions and run an instrumented force walk
  * that counts node visits (exact walk: per body; group walk: per group) and
  * the interactions evaluated over all bodies: with a node's multipole
- * (monopole, or monopole + quadrupole) and with single bodies (for
- * rooflines).  Leaves acc[] holding the forces; does not integrate. */
+ * (monopole, or monopole + quadrupole) and with single bodies, and the
+ * (node, group) pairs that went through the far-field local expansion (for
+ * rooflines; any pointer may be NULL).  Leaves acc[] holding the forces;
+ * does not integrate. */
 int bh_walk_stats(bh_sim* sim, uint64_t* node_visits, uint64_t* multipole_interactions,
-                  uint64_t* body_interactions);
+                  uint64_t* body_interactions, uint64_t* far_nodes);
 
 /* ---- differentiation (extension; no reference counterpart) ---------------- */
 /* Vector-Jacobian product of the force at the current positions: given

@@ -463,6 +463,87 @@ void orc_quadrupoles(uint32_t n, const uint32_t* left, const uint32_t* right, co
     free(seen);
 }
 
+/* Far field of the group walk (no reference counterpart): a node's
+ * potential Phi = -[M g + 1/2 (Sxx g_xx + 2 Sxy g_xy + Syy g_yy)] with the
+ * softened kernel g(R) = (|R|^2 + eps^2)^-1/2 is expanded about the group's
+ * box centre.  d^(a,b) g = s^(a+b+1) P_ab(rho), s = (|R|^2 + eps^2)^-1/2,
+ * rho = s R, with P_ab = sum_i sum_j c(a,i) c(b,j) rho_x^(a-2i) rho_y^(b-2j)
+ * w(a+b-i-j), c(a,i) = a!/(i! (a-2i)! 2^i), w(m) = (-1)^m (2m-1)!!.  The
+ * coefficients scaled by the length lambda (the box's half-diagonal),
+ * C_ab = lambda^(a+b) d^(a,b) Phi for 1 <= a+b <= 4, are summed over the far
+ * nodes; a body at x_g + lambda d feels
+ *   a_x = -(1/lambda) sum_{a+b<=3} C_(a+1)b d_x^a d_y^b/(a! b!),  a_y likewise. */
+#define ORC_FAR_COEFFS 14
+
+static int far_index(int a, int b) { return (a + b - 1) * (a + b + 2) / 2 + b; }
+
+static float fact_f(int k) {
+    float v = 1.0f;
+    for (int i = 2; i <= k; ++i) v *= (float)i;
+    return v;
+}
+
+static float far_poly_c(int a, int b, const float* px, const float* py) {
+    float acc = 0.0f;
+    for (int i = 0; 2 * i <= a; ++i) {
+        const float ca = fact_f(a) / (fact_f(i) * fact_f(a - 2 * i) * (float)(1 << i));
+        for (int j = 0; 2 * j <= b; ++j) {
+            const float cb = fact_f(b) / (fact_f(j) * fact_f(b - 2 * j) * (float)(1 << j));
+            const int m = a + b - i - j;
+            float w = 1.0f;
+            for (int k = 1; k <= m; ++k) w *= -(float)(2 * k - 1);
+            acc += ca * cb * w * (px[a - 2 * i] * py[b - 2 * j]);
+        }
+    }
+    return acc;
+}
+
+/* Add the scaled coefficients of one node (COM offset R = x_g - c) to C. */
+static void far_add_node(float* C, float rx, float ry, float m, float sxx, float sxy, float syy,
+                         float lambda, float eps2) {
+    const float u = (rx * rx + ry * ry) + eps2;
+    const float s = (float)(1.0 / sqrt((double)u));
+    float px[7], py[7];
+    px[0] = 1.0f;
+    py[0] = 1.0f;
+    px[1] = rx * s;
+    py[1] = ry * s;
+    for (int k = 2; k < 7; ++k) {
+        px[k] = px[k - 1] * px[1];
+        py[k] = py[k - 1] * py[1];
+    }
+    const float t = lambda * s, s2 = s * s;
+    const float qxx = s2 * sxx, qxy = s2 * sxy, qyy = s2 * syy;
+    for (int o = 1; o <= 4; ++o) {
+        float st = s;
+        for (int k = 0; k < o; ++k) st *= t;
+        for (int b = 0; b <= o; ++b) {
+            const int a = o - b;
+            const float quad = qxx * far_poly_c(a + 2, b, px, py) +
+                               2.0f * qxy * far_poly_c(a + 1, b + 1, px, py) +
+                               qyy * far_poly_c(a, b + 2, px, py);
+            const float v = m * far_poly_c(a, b, px, py) + 0.5f * quad;
+            C[far_index(a, b)] -= st * v;
+        }
+    }
+}
+
+/* The expansion's force at d (without the factor -1/lambda). */
+static void far_force(const float* C, float dx, float dy, float* fx, float* fy) {
+    float x = 0.0f, y = 0.0f;
+    for (int a = 0; a <= 3; ++a)
+        for (int b = 0; a + b <= 3; ++b) {
+            float mono = 1.0f;
+            for (int k = 0; k < a; ++k) mono *= dx;
+            for (int k = 0; k < b; ++k) mono *= dy;
+            mono /= fact_f(a) * fact_f(b);
+            x += C[far_index(a + 1, b)] * mono;
+            y += C[far_index(a, b + 1)] * mono;
+        }
+    *fx = x;
+    *fy = y;
+}
+
 void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const float* mass,
                     const float* pos, const float* com, const float* mass_node, const float* aabb,
                     const float* quad, const uint32_t* left, const uint32_t* right, float* acc) {
@@ -507,6 +588,7 @@ void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const 
         uint32_t* nodes = (uint32_t*)malloc(sizeof(uint32_t) * cap);
         uint32_t* rfirst = (uint32_t*)malloc(sizeof(uint32_t) * cap);
         uint32_t* rcount = (uint32_t*)malloc(sizeof(uint32_t) * cap);
+        uint32_t* fars = (uint32_t*)malloc(sizeof(uint32_t) * cap);
 #define ORC_GROW(need)                                                         \
         if ((size_t)(need) > cap) {                                            \
             cap = 2 * cap > (size_t)(need) ? 2 * cap : (size_t)(need);         \
@@ -514,6 +596,7 @@ void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const 
             nodes = (uint32_t*)realloc(nodes, sizeof(uint32_t) * cap);         \
             rfirst = (uint32_t*)realloc(rfirst, sizeof(uint32_t) * cap);       \
             rcount = (uint32_t*)realloc(rcount, sizeof(uint32_t) * cap);       \
+            fars = (uint32_t*)realloc(fars, sizeof(uint32_t) * cap);           \
         }
 #pragma omp for schedule(dynamic, 1)
         for (int64_t g = 0; g < (int64_t)ngroups; ++g) {
@@ -525,13 +608,20 @@ void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const 
                 lox = fminf(lox, pos[2 * b]); hix = fmaxf(hix, pos[2 * b]);
                 loy = fminf(loy, pos[2 * b + 1]); hiy = fmaxf(hiy, pos[2 * b + 1]);
             }
-            size_t nn_ = 0, nr = 0;
+            /* far field: box centre and squared half-diagonal */
+            const float gcx = 0.5f * (lox + hix), gcy = 0.5f * (loy + hiy);
+            const float ghx = hix - lox, ghy = hiy - loy;
+            const float rg2 = 0.25f * (ghx * ghx + ghy * ghy);
+            const float fa2 = p->far_alpha * p->far_alpha;
+            const int far_on = plummer && p->multipole >= 2 && fa2 > 0.0f && rg2 > 0.0f;
+            size_t nn_ = 0, nr = 0, nf = 0;
             int64_t sp = 0;
             if (n > 1) stack[sp++] = 0;
             while (sp > 0) {
                 ORC_GROW((size_t)sp + 2);
                 ORC_GROW(nn_ + 1);
                 ORC_GROW(nr + 1);
+                ORC_GROW(nf + 1);
                 const uint32_t v = stack[--sp];
                 if (v >= nm1) { rfirst[nr] = v - nm1; rcount[nr++] = 1; continue; }
                 const float* bx = &aabb[4 * (size_t)v];
@@ -545,7 +635,9 @@ void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const 
                 const float sx = fmaxf(bx[0] - hix, lox - bx[2]);
                 const float sy = fmaxf(bx[1] - hiy, loy - bx[3]);
                 if (Ls * Ls < th2 * d2 && (sx > 0.0f || sy > 0.0f)) {
-                    nodes[nn_++] = v;
+                    const float ox = cx - gcx, oy = cy - gcy;
+                    if (far_on && rg2 < fa2 * (ox * ox + oy * oy)) fars[nf++] = v;
+                    else nodes[nn_++] = v;
                 } else if (last[v] - first[v] + 1 <= L) {
                     rfirst[nr] = first[v];
                     rcount[nr++] = last[v] - first[v] + 1;
@@ -554,10 +646,25 @@ void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const 
                     stack[sp++] = left[v];
                 }
             }
+            float C[ORC_FAR_COEFFS] = {0};
+            const float lam = far_on ? sqrtf(rg2) : 1.0f;
+            for (size_t j = 0; j < nf; ++j) {
+                const uint32_t v = fars[j];
+                far_add_node(C, gcx - com[2 * (size_t)v], gcy - com[2 * (size_t)v + 1],
+                             mass_node[v], quad[3 * (size_t)v], quad[3 * (size_t)v + 1],
+                             quad[3 * (size_t)v + 2], lam, eps2);
+            }
             for (uint32_t s = base; s < end; ++s) {
                 const uint32_t b = ids[s];
                 const float x = pos[2 * b], y = pos[2 * b + 1], m1 = mass[b];
                 float ax = 0.0f, ay = 0.0f;
+                if (nf > 0) {
+                    const float il = 1.0f / lam;
+                    float fx, fy;
+                    far_force(C, (x - gcx) * il, (y - gcy) * il, &fx, &fy);
+                    ax = -(fx * il);
+                    ay = -(fy * il);
+                }
                 for (size_t j = 0; j < nn_; ++j) {
                     const uint32_t v = nodes[j];
                     const float m2 = mass_node[v];
@@ -605,6 +712,7 @@ void orc_walk_group(const orc_params* p, uint32_t n, const uint32_t* ids, const 
         free(nodes);
         free(rfirst);
         free(rcount);
+        free(fars);
     }
     free(gfirst);
     free(gcount);

@@ -57,6 +57,7 @@ typedef struct orc_params {
     int walk_mode;            /* 0 = reference per-body walk, 1 = group walk (extension) */
     int multipole;            /* group walk: 1 monopole, 2 monopole + quadrupole */
     int bodies_per_lane;      /* group walk: group = 32 * bodies_per_lane consecutive sorted slots */
+    float far_alpha;          /* group walk, Plummer: far nodes through a local expansion (0 = off) */
 } orc_params;
 
 /* Domain used by the Morton encode: scale/offset for 32-bit keys, or the

@@ -36,6 +36,7 @@ class OrcParams(ctypes.Structure):
         ("walk_mode", ctypes.c_int),
         ("multipole", ctypes.c_int),
         ("bodies_per_lane", ctypes.c_int),
+        ("far_alpha", ctypes.c_float),
     ]
 
 
@@ -110,10 +111,10 @@ def _p(a):
 def params(G=1.0, dt=0.1 / 60.0, eps_mult=1.0, theta=0.6, softening="reference",
            plummer_eps=1e-3, morton_bits=32, morton_domain="fixed2000",
            integrator="symplectic-euler", leaf_size=1, threads=0, walk="exact", multipole=2,
-           bodies_per_lane=2) -> OrcParams:
+           bodies_per_lane=2, far_alpha=0.0) -> OrcParams:
     return OrcParams(G, dt, eps_mult, theta, SOFT[softening], plummer_eps, morton_bits,
                      DOMAIN[morton_domain], INTEGRATOR[integrator], leaf_size, threads,
-                     WALK[walk], multipole, bodies_per_lane)
+                     WALK[walk], multipole, bodies_per_lane, far_alpha)
 
 
 def params_from_config(cfg, threads: int = 0) -> OrcParams:
@@ -123,7 +124,8 @@ def params_from_config(cfg, threads: int = 0) -> OrcParams:
                   morton_bits=cfg.mortonBits, morton_domain=cfg.mortonDomain,
                   integrator=cfg.integrator, leaf_size=cfg.leafSize, threads=threads,
                   walk=getattr(cfg, "walk", "exact"), multipole=getattr(cfg, "multipole", 2),
-                  bodies_per_lane=getattr(cfg, "bodiesPerLane", 2) or 2)
+                  bodies_per_lane=getattr(cfg, "bodiesPerLane", 2) or 2,
+                  far_alpha=getattr(cfg, "farAlpha", 0.0))
 
 
 def f32(a, shape=None):

@@ -283,6 +283,61 @@ def test_group_walk_small_n(bh, orc, n):
     sim.close()
 
 
+@pytest.mark.parametrize("bpl", [1, 2, 4])
+@pytest.mark.parametrize("alpha", [0.25, 0.5])
+def test_group_walk_far_field_matches_oracle(bh, orc, bpl, alpha):
+    # Far nodes through the group's local expansion: the same lists and
+    # expansions as the oracle's restatement (FP32 sums in another order;
+    # far/near flips where a node's COM differs in its last bit), and the
+    # same accuracy against the FP64 direct sum.
+    sim = make_sim(bh, 30000, "colliding-disks", seed=3,
+                   **dict(GROUP, bodiesPerLane=bpl, farAlpha=alpha))
+    acc, acc_ref = compare_tree(orc, sim)
+    err = acc_errors(acc, acc_ref)
+    assert np.median(err) <= 1e-5
+    assert err.max() <= 1e-3
+    visits, multi, body, far = sim.walk_stats()
+    assert far > 0
+    mass, pos, _ = sim.download()
+    fe = sim.forceError(acc, nsample=2000, seed=4)
+    sample = np.sort(np.random.default_rng(4).choice(30000, 2000, replace=False))
+    ref64 = orc.direct_sum_fp64(orc.params_from_config(sim.config), mass, pos, sample)
+    e_orc = np.linalg.norm(acc_ref[sample] - ref64, axis=1) / np.linalg.norm(ref64, axis=1)
+    assert abs(fe["median"] - np.median(e_orc)) <= 0.02 * np.median(e_orc)
+    sim.close()
+
+
+def test_group_walk_far_field_steps_and_ensemble(bh, orc):
+    # The far field inside captured steps (leapfrog) against the oracle, and
+    # on an ensemble (each group's expansion sums only its own system).
+    sim = make_sim(bh, 20000, "colliding-disks", seed=8,
+                   **dict(GROUP, integrator="leapfrog-kdk", deltaTime=5e-5, farAlpha=0.3))
+    mass, pos, vel = sim.download()
+    st = orc.State(oracle_params(orc, sim), mass, pos, vel)
+    sim.step(4)
+    sim.sync()
+    st.step(4)
+    _, p_gpu, v_gpu = sim.download()
+    p_ref, v_ref = st.state()
+    assert np.abs(v_gpu - v_ref).max() <= 1e-4 * np.abs(v_ref).max()
+    assert np.abs(p_gpu - p_ref).max() <= 1e-5 * (np.abs(p_ref).max() + 1)
+    sim.close()
+    sizes = [3000, 700, 5000]
+    ens = bh.Ensemble(sizes, bh.Config(**dict(GROUP, farAlpha=0.3)))
+    ens.setScenarios(None, seed=3)
+    m2, p2, v2 = ens.download()
+    acc = ens.computeAccelerations()
+    off = ens.offsets
+    p = orc.params_from_config(ens.config)
+    for k in range(len(sizes)):
+        sl = slice(int(off[k]), int(off[k + 1]))
+        ref = orc.State(p, m2[sl], p2[sl], v2[sl]).accelerations()
+        e = acc_errors(acc[sl], ref)
+        assert np.median(e) <= 1e-5, (k, np.median(e))
+        assert e.max() <= 1e-3, (k, e.max())
+    ens.close()
+
+
 def test_group_walk_reference_softening(bh, orc):
     sim = make_sim(bh, 20000, "default", seed=6, walk="group", bhTheta=0.5, leafSize=4)
     acc, acc_ref = compare_tree(orc, sim)
@@ -330,14 +385,19 @@ def test_group_walk_kdk_steps_match_oracle(bh, orc):
 
 def test_walk_stats_counts(bh):
     sim = make_sim(bh, 50000, "colliding-disks", seed=2, **GROUP)
-    visits, multi, body = sim.walk_stats()
-    assert visits > 0 and multi > 0 and body > 0
+    visits, multi, body, far = sim.walk_stats()
+    assert visits > 0 and multi > 0 and body > 0 and far == 0
     sim2 = make_sim(bh, 50000, "colliding-disks", seed=2, softening="plummer", bhTheta=0.5,
                     mortonDomain="bbox")
-    v2, m2, b2 = sim2.walk_stats()
-    assert v2 > 0 and m2 > 0 and b2 > 0
+    v2, m2, b2, f2 = sim2.walk_stats()
+    assert v2 > 0 and m2 > 0 and b2 > 0 and f2 == 0
+    # with the far field, far (node, group) pairs replace part of the multipole ones
+    sim3 = make_sim(bh, 50000, "colliding-disks", seed=2, **dict(GROUP, farAlpha=0.25))
+    v3, m3, b3, f3 = sim3.walk_stats()
+    assert f3 > 0 and m3 < multi and b3 == body
     sim.close()
     sim2.close()
+    sim3.close()
 
 
 def test_autotune_picks_a_valid_config_and_stays_accurate(bh, orc):

@@ -52,7 +52,8 @@ class bh_config(ctypes.Structure):
         ("walk_mode", ctypes.c_int32),
         ("multipole_order", ctypes.c_int32),
         ("bodies_per_lane", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("far_alpha", ctypes.c_float),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
 
@@ -125,6 +126,7 @@ SIGNATURES = {
                                       ctypes.POINTER(ctypes.c_uint32)]),
     "bh_kernels_per_step": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint32)]),
     "bh_walk_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64),
+                                     ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_uint64)]),
     "bh_ensemble_create": (ctypes.c_int, [ctypes.POINTER(bh_config), _P, ctypes.c_uint32,

@@ -33,6 +33,8 @@ class Config:
     walk: str = "exact"                 # "exact" (reference per-body walk) | "group"
     multipole: int = 2                  # group walk: 1 monopole, 2 + quadrupole
     bodiesPerLane: int = 2              # group walk: group = 32 x bodiesPerLane bodies
+    farAlpha: float = 0.0               # group walk, Plummer: far nodes (r_g < farAlpha R)
+                                        # act through one local expansion per group (0 = off)
 
     def to_c(self, device: int = 0) -> _lib.bh_config:
         c = _lib.bh_config()
@@ -57,6 +59,7 @@ class Config:
         c.walk_mode = {"exact": _lib.BH_WALK_EXACT, "group": _lib.BH_WALK_GROUP}[self.walk]
         c.multipole_order = self.multipole
         c.bodies_per_lane = self.bodiesPerLane
+        c.far_alpha = self.farAlpha
         return c
 
 

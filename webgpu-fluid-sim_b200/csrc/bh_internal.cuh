@@ -126,6 +126,10 @@ struct WalkParams {
     // stack entries a warp may use (0 = the kernel's full capacity); a test
     // lowers it to make the overflow check trip
     int stack_cap = 0;
+    // group walk, Plummer softening: far_alpha^2 (0 = no far field); an
+    // accepted node with r_g^2 < far_alpha^2 R^2 goes through the group's
+    // local expansion (far_field.cuh)
+    float far_alpha2 = 0.0f;
 };
 
 // Per-step scratch that must start at zero.  One memset clears it.

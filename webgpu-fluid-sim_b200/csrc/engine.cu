@@ -191,6 +191,8 @@ static int validate_config(bh_sim* s, const bh_config& c) {
     if (c.walk_mode == BH_WALK_GROUP && c.bodies_per_lane != 0 && c.bodies_per_lane != 1 &&
         c.bodies_per_lane != 2 && c.bodies_per_lane != 4)
         return fail(s, BH_ERR_INVALID_ARGUMENT, "bodies_per_lane must be 1, 2 or 4");
+    if (!(c.far_alpha >= 0.0f && c.far_alpha <= 0.5f))
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "far_alpha must be in [0, 0.5]");
     if (!(c.delta_time == c.delta_time) || !(c.bh_theta >= 0.0f))
         return fail(s, BH_ERR_INVALID_ARGUMENT, "delta_time must be a number and bh_theta >= 0");
     return BH_OK;
@@ -411,6 +413,7 @@ static bh::WalkParams walk_params(const bh_sim* s, int mode) {
     p.slot_lo = integrating ? s->shard_lo : 0u;
     p.slot_hi = integrating ? s->shard_hi : 0xFFFFFFFFu;
     p.stack_cap = (int)s->debug_stack_cap;
+    p.far_alpha2 = c.walk_mode == BH_WALK_GROUP ? c.far_alpha * c.far_alpha : 0.0f;
     return p;
 }
 
@@ -1019,6 +1022,9 @@ static int adjoint_supported(bh_sim* s) {
                     "the adjoint needs the group walk and Plummer softening");
     if (s->b.num_systems > 0)
         return fail(s, BH_ERR_NOT_SUPPORTED, "the adjoint runs on single systems, not ensembles");
+    if (s->cfg.far_alpha > 0.0f)
+        return fail(s, BH_ERR_NOT_SUPPORTED,
+                    "the adjoint differentiates the walk without the far field (far_alpha = 0)");
     return BH_OK;
 }
 
@@ -1214,9 +1220,9 @@ extern "C" int bh_rollout_grad(bh_sim* s, uint32_t steps, uint32_t checkpoint_ev
 }
 
 extern "C" int bh_walk_stats(bh_sim* s, uint64_t* node_visits, uint64_t* multipole_interactions,
-                             uint64_t* body_interactions) {
+                             uint64_t* body_interactions, uint64_t* far_nodes) {
     BH_HANDLE(s);
-    unsigned long long h[3] = {0, 0, 0};
+    unsigned long long h[4] = {0, 0, 0, 0};
     if (s->b.n > 0) {
         enqueue_tree(s, [](int) {});
         bh::WalkParams p = walk_params(s, bh::kWalkForces);
@@ -1232,6 +1238,7 @@ extern "C" int bh_walk_stats(bh_sim* s, uint64_t* node_visits, uint64_t* multipo
     if (node_visits) *node_visits = h[0];
     if (multipole_interactions) *multipole_interactions = h[1];
     if (body_interactions) *body_interactions = h[2];
+    if (far_nodes) *far_nodes = h[3];
     return check_device_errors(s);
 }
 

@@ -15,11 +15,12 @@
 // stack entries that stand for both children of an opened node -- adjacent
 // in the Karras numbering, one round trip for the pair -- which halve the
 // dependent steps but double the emission work per step and the registers.)  The group
-// opens a node unless
+// accepts a node when
 //     L^2 < theta^2 d^2,  L = longest side of the node's box,
-//     d = distance between the group's box and the node's box,
-// which is stricter for every body of the group than the per-body test
-// length / |com - x| < theta.  Accepted nodes act through their monopole and
+//     d = distance from the group's box to the node's COM,
+// and the node's box lies apart from the group's box (group_accepts); then
+// every body of the group meets the per-body test length / |com - x| <
+// theta.  Other nodes are opened.  Accepted nodes act through their monopole and
 // (multipole order 2) quadrupole about the COM,
 //     a = G [ M r/|r|^3 - Q'r/|r|^5 + 5/2 (r.Q'r) r/|r|^7 ],  Q' = 3S - tr(S) I,
 // with r = com - x and |r|^2 = r.r + eps^2 (S = second moments about the COM).
@@ -44,7 +45,16 @@
 // yields ready operand pairs, and with the quadrupole negated so every
 // accumulation is a plain fused multiply-add.  With eps^2 > 0 a body's own
 // leaf adds exactly zero (r = 0), so no self test is needed.
+//
+// Far field (far_alpha > 0, extension): an accepted node whose COM lies far
+// from the group compared with the group's size (r_g < far_alpha R, r_g the
+// group box's half-diagonal, R the distance from the box centre to the COM)
+// is not evaluated body by body.  Lanes turn 32 such nodes at a time into
+// the coefficients of a local expansion about the box centre, each lane
+// summing its own in registers; at the end of the group the lanes' sums are
+// reduced and every body evaluates the expansion once (far_field.cuh).
 #include "bh_internal.cuh"
+#include "far_field.cuh"
 #include "packed.cuh"
 
 namespace bh {
@@ -54,32 +64,57 @@ constexpr int kWalkStack = 384;               // per-warp stack entries
 constexpr int kWalkDfsAt = kWalkStack - 128;  // >= 32 + 96 below the capacity
 
 constexpr int kSlotList = 32 + 32 * kGroupMaxLeaf;  // body slots: < 32 kept + one step's adds
-
+// Node list entries.  Without the far field the multipole list is flushed
+// at 32 entries, so it holds < 64 after any step.  With it, multipole
+// entries grow from the bottom and far entries from the top; both lists are
+// flushed at 32 entries, so before a step each holds < 32 and one step adds
+// at most 32 in all: < 96 together.
+template <bool FAR>
 struct GroupSmem {
+    static constexpr int kListCap = FAR ? 96 : kGroupList;
     uint32_t stack[kWalkStack];
     // node entry j: ent[j][0] = {cx, cx, cy, cy}, ent[j][1] = {m, m, -Q'xx, -Q'xx},
     //               ent[j][2] = {-Q'xy, -Q'xy, -Q'yy, -Q'yy}
-    float4 ent[kGroupList][3];
+    // far entry j (at kListCap - 1 - j): {cx, cy, m, Sxx}, {Sxy, Syy, 0, 0}
+    float4 ent[kListCap][3];
     uint32_t slot[kSlotList];  // sorted slots of bodies to sum one by one
     float4 body[32][2];        // 32 staged leaf records as pairs {x,x,y,y}, {m,m,0,0}
 };
+
+// Far list: the top `cnt` (<= 32) far entries of `nf_total`, one per lane,
+// added to the lane's local-expansion sums.
+__device__ __forceinline__ void far_batch(GroupSmem<true>& S, float (&cacc)[kFarCoeffs], int lane,
+                                          int nf_total, int cnt, float gcx, float gcy, float lam,
+                                          float eps2) {
+    constexpr int cap = GroupSmem<true>::kListCap;
+    if (lane < cnt) {
+        const int j = nf_total - cnt + lane;
+        const float4 a = S.ent[cap - 1 - j][0];
+        const float4 b = S.ent[cap - 1 - j][1];
+        far_node_coeffs(cacc, __fsub_rn(gcx, a.x), __fsub_rn(gcy, a.y), a.z, a.w, b.x, b.y, lam,
+                        eps2);
+    }
+    __syncwarp();
+}
 
 // Resident blocks per SM the register budget is sized for (measured best:
 // 6 for groups of <= 64 bodies; 5 for 128-body groups, whose two packed
 // accumulator pairs per lane need more registers).
 constexpr int walk_min_blocks(int bpl) { return bpl >= 4 ? 5 : 6; }
 
-template <int BPL, int MP, bool PLUMMER>
+// FAR: the far-field variant (Plummer softening, quadrupoles); the other
+// instantiations carry none of its code or registers.
+template <int BPL, int MP, bool PLUMMER, bool FAR>
 __global__ void __launch_bounds__(kGroupWarps * 32, walk_min_blocks(BPL))
 walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ node4,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ ids,
                   float2* __restrict__ pos, float2* __restrict__ vel, float2* __restrict__ acc,
                   const WalkParams P, uint32_t* __restrict__ err) {
     constexpr int NP = BPL / 2;  // packed pairs per lane (BPL >= 2)
-    __shared__ GroupSmem smem[kGroupWarps];
+    __shared__ GroupSmem<FAR> smem[kGroupWarps];
     if (step_failed(err)) return;  // the tree of this step was not built
     const int lane = threadIdx.x & 31;
-    GroupSmem& S = smem[threadIdx.x >> 5];
+    GroupSmem<FAR>& S = smem[threadIdx.x >> 5];
     const unsigned FULL = 0xFFFFFFFFu;
     const unsigned lt = (1u << lane) - 1u;
     const uint32_t n = P.n, nm1 = n - 1;
@@ -89,7 +124,7 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
     // With a positive softening the own-leaf term is exactly zero.
     const bool self_test = !(PLUMMER && eps2 > 0.0f);
     const bool counting = P.count != 0;
-    unsigned long long c_vis = 0, c_node = 0, c_body = 0;
+    unsigned long long c_vis = 0, c_node = 0, c_body = 0, c_far = 0;
     const int stack_cap = (P.stack_cap > 0 && P.stack_cap < kWalkStack) ? P.stack_cap : kWalkStack;
 
     while (true) {
@@ -135,6 +170,18 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
             ghix = fmaxf(ghix, __shfl_xor_sync(FULL, ghix, o));
             ghiy = fmaxf(ghiy, __shfl_xor_sync(FULL, ghiy, o));
         }
+        // Far field: box centre, squared half-diagonal and its square root
+        // (the expansion's length scale); off for a group of coincident bodies.
+        const float gcx = __fmul_rn(0.5f, __fadd_rn(glox, ghix));
+        const float gcy = __fmul_rn(0.5f, __fadd_rn(gloy, ghiy));
+        const float ghx = __fsub_rn(ghix, glox), ghy = __fsub_rn(ghiy, gloy);
+        const float rg2 = __fmul_rn(0.25f, __fadd_rn(__fmul_rn(ghx, ghx), __fmul_rn(ghy, ghy)));
+        const bool far_on = FAR && PLUMMER && P.far_alpha2 > 0.0f && rg2 > 0.0f;
+        const float lam = far_on ? __fsqrt_rn(rg2) : 1.0f;
+        bool far_used = false;
+        float cacc[kFarCoeffs];  // this lane's local-expansion sums
+#pragma unroll
+        for (int k = 0; k < kFarCoeffs; ++k) cacc[k] = 0.0f;
         // Accumulators: packed pairs (BPL >= 2) or scalars (BPL == 1).
         f2x X[NP > 0 ? NP : 1], Y[NP > 0 ? NP : 1], AX[NP > 0 ? NP : 1], AY[NP > 0 ? NP : 1];
         float ax1 = 0.f, ay1 = 0.f;
@@ -253,8 +300,7 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
             }
             __syncwarp();
         };
-
-        int sp = 0, nn = 0, ns = 0;
+        int sp = 0, nn = 0, ns = 0, nf = 0;
         if (n > 1) {
             if (lane == 0) S.stack[0] = 0u;
             sp = 1;
@@ -303,6 +349,24 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
                         r1 = lk.y;
                     }
                 }
+            }
+            // Far field: an accepted node far from the group goes to the far list.
+            bool emit_far = false;
+            if (far_on && emit_node) {
+                const float rx = __fsub_rn(mom.x, gcx), ry = __fsub_rn(mom.y, gcy);
+                const float R2 = __fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry));
+                emit_far = rg2 < __fmul_rn(P.far_alpha2, R2);
+                emit_node = !emit_far;
+            }
+            if (FAR && far_on) {
+                const unsigned mf = __ballot_sync(FULL, emit_far);
+                if (emit_far) {
+                    const int q = GroupSmem<FAR>::kListCap - 1 - (nf + __popc(mf & lt));
+                    const bool quad = MP >= 2;
+                    S.ent[q][0] = make_float4(mom.x, mom.y, mom.z, quad ? sq.x : 0.f);
+                    S.ent[q][1] = make_float4(quad ? sq.y : 0.f, quad ? sq.z : 0.f, 0.f, 0.f);
+                }
+                nf += __popc(mf);
             }
             const unsigned mn = __ballot_sync(FULL, emit_node);
             if (emit_node) {
@@ -358,6 +422,14 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
                 eval_bodies(ns);
                 ns = 0;
             }
+            if constexpr (FAR) {
+                if (nf >= 32) {
+                    far_batch(S, cacc, lane, nf, 32, gcx, gcy, lam, eps2);
+                    if (counting) c_far += 32ull;
+                    nf -= 32;
+                    far_used = true;
+                }
+            }
         }
         if (nn > 0) {
             eval_nodes(nn);
@@ -367,7 +439,44 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
             if (counting) c_body += (unsigned long long)ns * nvalid;
             eval_bodies(ns);
         }
+        if constexpr (FAR) {
+            if (nf > 0) {
+                far_batch(S, cacc, lane, nf, nf, gcx, gcy, lam, eps2);
+                if (counting) c_far += (unsigned long long)nf;
+                far_used = true;
+            }
+        }
         if (counting && n > 1) c_body -= nvalid;  // each body met its own leaf once
+        __syncwarp();
+        // Far field: reduce the lane columns (every lane gets the sums) and
+        // evaluate the local expansion at each of the lane's bodies.
+        float fx[BPL], fy[BPL];
+#pragma unroll
+        for (int k = 0; k < BPL; ++k) {
+            fx[k] = 0.0f;
+            fy[k] = 0.0f;
+        }
+        if (far_used) {
+            float c[kFarCoeffs];
+#pragma unroll
+            for (int k = 0; k < kFarCoeffs; ++k) {
+                float v = cacc[k];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+                c[k] = v;
+            }
+            const float inv_lam = __fdiv_rn(1.0f, lam);
+#pragma unroll
+            for (int k = 0; k < BPL; ++k) {
+                if ((uint32_t)k * 32u + (uint32_t)lane >= nvalid) continue;
+                const float dx = __fmul_rn(__fsub_rn(bx[k], gcx), inv_lam);
+                const float dy = __fmul_rn(__fsub_rn(by[k], gcy), inv_lam);
+                float ex, ey;
+                far_eval(c, dx, dy, ex, ey);
+                fx[k] = -__fmul_rn(ex, inv_lam);
+                fy[k] = -__fmul_rn(ey, inv_lam);
+            }
+        }
         __syncwarp();
 
         // Integrate (same modes as the exact walk).
@@ -386,7 +495,9 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
         for (int k = 0; k < BPL; ++k) {
             const uint32_t s = base + (uint32_t)k * 32u + (uint32_t)lane;
             if ((uint32_t)k * 32u + (uint32_t)lane >= nvalid) continue;
-            const float gx = P.g * ax[k], gy = P.g * ay[k];
+            const float axk = far_used ? __fadd_rn(ax[k], fx[k]) : ax[k];
+            const float ayk = far_used ? __fadd_rn(ay[k], fy[k]) : ay[k];
+            const float gx = P.g * axk, gy = P.g * ayk;
             const uint32_t b = __ldg(&ids[s]);
             if (P.mode == kWalkForces) {
                 acc[b] = make_float2(gx, gy);
@@ -411,17 +522,18 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
         atomicAdd(&P.counters[0], c_vis);
         atomicAdd(&P.counters[1], c_node);
         atomicAdd(&P.counters[2], c_body);
+        atomicAdd(&P.counters[3], c_far);
     }
 }
 
-template <int BPL, int MP, bool PL>
+template <int BPL, int MP, bool PL, bool FAR = false>
 static void launch_t(const DeviceBuffers& b, const WalkParams& p, cudaStream_t s) {
     static int blocks_per_sm[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     int& bps = blocks_per_sm[dev & 63];
     if (bps == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, walk_group_kernel<BPL, MP, PL>,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, walk_group_kernel<BPL, MP, PL, FAR>,
                                                       kGroupWarps * 32, 0);
         if (bps < 1) bps = 1;
     }
@@ -432,14 +544,16 @@ static void launch_t(const DeviceBuffers& b, const WalkParams& p, cudaStream_t s
     const uint32_t need = (b.n + kGroupWarps - 1) / kGroupWarps;
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
-    walk_group_kernel<BPL, MP, PL><<<blocks, kGroupWarps * 32, 0, s>>>(
+    walk_group_kernel<BPL, MP, PL, FAR><<<blocks, kGroupWarps * 32, 0, s>>>(
         b.gnode, b.node4, b.groups, b.ids, b.pos, b.vel, b.acc, p, b.err);
 }
 
 template <int BPL>
 static void launch_bpl(const DeviceBuffers& b, const WalkParams& p, cudaStream_t s) {
     if (p.multipole >= 2) {
-        if (p.plummer) launch_t<BPL, 2, true>(b, p, s); else launch_t<BPL, 2, false>(b, p, s);
+        if (p.plummer && p.far_alpha2 > 0.0f) launch_t<BPL, 2, true, true>(b, p, s);
+        else if (p.plummer) launch_t<BPL, 2, true>(b, p, s);
+        else launch_t<BPL, 2, false>(b, p, s);
     } else {
         if (p.plummer) launch_t<BPL, 1, true>(b, p, s); else launch_t<BPL, 1, false>(b, p, s);
     }

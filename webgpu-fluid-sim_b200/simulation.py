@@ -250,14 +250,16 @@ class Simulation:
                                               ctypes.byref(loss), _ptr(gx), _ptr(gv), _ptr(gm)))
         return float(loss.value), gx, gv, gm
 
-    def walk_stats(self) -> tuple[int, int, int]:
-        """(node visits, multipole interactions, body interactions) at the current positions."""
+    def walk_stats(self) -> tuple[int, int, int, int]:
+        """(node visits, multipole interactions, body interactions, far-field
+        (node, group) pairs) at the current positions."""
         v = ctypes.c_uint64()
         m = ctypes.c_uint64()
         b = ctypes.c_uint64()
+        f = ctypes.c_uint64()
         self._check(self._lib.bh_walk_stats(self._h, ctypes.byref(v), ctypes.byref(m),
-                                            ctypes.byref(b)))
-        return int(v.value), int(m.value), int(b.value)
+                                            ctypes.byref(b), ctypes.byref(f)))
+        return int(v.value), int(m.value), int(b.value), int(f.value)
 
     def diagnostics(self, potential: bool = True) -> dict:
         """FP64 conserved quantities of the current state (bh_diagnostics_compute):
