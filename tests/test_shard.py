@@ -132,6 +132,63 @@ def test_emulated_ranks_equal_one_gpu(bh, world, mode):
         s.close()
 
 
+def _gloo_sharded_rank(rank, world, port, mode, n, steps, q):
+    # One rank of a sharded run: its own process and CUDA context on the one
+    # GPU; the all-gather goes through gloo on the host, so no kernel waits
+    # on another rank.
+    import datetime
+    import importlib
+    import sys
+    import torch.distributed as dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    try:
+        bh = importlib.import_module("webgpu-fluid-sim_b200")
+        dist.init_process_group("gloo", rank=rank, world_size=world,
+                                timeout=datetime.timedelta(seconds=60))
+        sh = bh.ShardedSimulation(bh.Config(**CFGS[mode]), n, "colliding-disks", seed=8)
+        sh.step(steps)
+        sh.sync()
+        mass, pos, vel = sh.download()
+        sh.close()
+        dist.barrier()
+        dist.destroy_process_group()
+        q.put((rank, True, (mass, pos, vel)))
+    except Exception as e:  # report instead of leaving the parent waiting
+        q.put((rank, False, repr(e)))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["leapfrog", "euler"])
+def test_sharded_simulation_two_gloo_processes_equal_one_gpu(bh, mode):
+    # ShardedSimulation end to end over two processes (gloo, chunks staged
+    # through host memory) against one unsharded Simulation, bit for bit.
+    import torch.multiprocessing as mp
+    n, steps = 40_001, 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gloo_sharded_rank, args=(r, 2, port, mode, n, steps, q))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all(ok for _, ok, _ in res), [r[2] for r in res if not r[1]]
+    ref = bh.Simulation(bh.Config(**CFGS[mode]))
+    ref.setNumBodies(n)
+    ref.setScenario("colliding-disks", 8)
+    ref.step(steps)
+    want = ref.download()
+    ref.close()
+    for rank, _, got in res:
+        for a, b in zip(got, want):
+            assert np.array_equal(a, b), f"rank {rank} differs from one GPU"
+
+
 @pytest.mark.gpu
 def test_sharded_simulation_world_one_equals_simulation(bh):
     cfg = bh.Config(**CFGS["leapfrog"])

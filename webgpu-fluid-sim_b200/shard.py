@@ -65,6 +65,14 @@ def all_gather_chunks(out, chunk, group=None) -> None:
         return
     if dist.get_backend(group) == "nccl":
         dist.all_gather_into_tensor(out.view(-1), chunk, group=group)
+    elif chunk.is_cuda:
+        # gloo gathers host tensors: the chunks cross host memory (on the
+        # current stream, so after the pack and before the unpack)
+        import torch
+        host = chunk.cpu()
+        parts = [torch.empty_like(host) for _ in range(out.shape[0])]
+        dist.all_gather(parts, host, group=group)
+        out.copy_(torch.stack(parts))
     else:
         dist.all_gather(list(out.unbind(0)), chunk, group=group)
 
