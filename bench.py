@@ -708,7 +708,7 @@ def run_own(args):
                 dist.broadcast_object_list(box, src=0)
                 tune = box[0]
             cfg = dataclasses.replace(cfg, bodiesPerLane=tune["bodiesPerLane"],
-                                      leafSize=tune["leafSize"])
+                                      leafSize=tune["leafSize"], walkBlock=tune["walkBlock"])
         sharded = pkg.ShardedSimulation(cfg, n, wl["scenario"], seed=1, device=local)
         sim = sharded.sim
     else:
@@ -806,6 +806,7 @@ def run_own(args):
                        "integrator": cfg.integrator, "morton_bits": cfg.mortonBits,
                        "walk": f"{cfg.walk}, multipole order {cfg.multipole}",
                        "bodies_per_lane": cfg.bodiesPerLane, "leaf_size": cfg.leafSize,
+                       "walk_block": cfg.walkBlock, "far_alpha": cfg.farAlpha,
                        "autotuned": tune is not None, "shape_pinned": bool(args.walk_shape),
                        "parallelism": (f"shard{world} (sorted-slot ranges, one all-gather of "
                                        f"16 B/body per step)" if sharded is not None else

@@ -222,12 +222,15 @@ typedef struct bh_tune_result {
     int32_t leaf_size;       /* chosen bucket size */
     float walk_ms;           /* its average walk time */
     int32_t candidates;      /* candidates timed */
+    int32_t walk_block;      /* chosen threads per walk block */
 } bh_tune_result;
 
 /* Time the group walk (on force evaluations at the current positions, which
  * do not advance the state) for bodies_per_lane in {1, 2, 4} x leaf_size in
- * {2, 4, 8}, `trials` launches each after one warm-up, and keep the fastest
- * in the handle's configuration.  Group walk only. */
+ * {2, 4, 8} with 128-thread blocks, then the best of those with 64- and
+ * 256-thread blocks (walk_block), `trials` launches each after one warm-up,
+ * and keep the fastest in the handle's configuration (11 candidates).
+ * Group walk only. */
 int bh_autotune(bh_sim* sim, uint32_t trials, bh_tune_result* out);
 
 /* The handle's current configuration (after bh_autotune, for instance). */

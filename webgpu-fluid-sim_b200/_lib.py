@@ -67,6 +67,7 @@ class bh_tune_result(ctypes.Structure):
         ("leaf_size", ctypes.c_int32),
         ("walk_ms", ctypes.c_float),
         ("candidates", ctypes.c_int32),
+        ("walk_block", ctypes.c_int32),
     ]
 
 

@@ -220,6 +220,8 @@ void launch_encode_ensemble(const DeviceBuffers& b, cudaStream_t s);
 void launch_zero_step(const DeviceBuffers& b, cudaStream_t s);  // scratch + sort status
 void launch_sort(const DeviceBuffers& b, cudaStream_t s);
 cudaError_t sort_init_attributes();
+// walk_group.cu: the group walk's dynamic shared memory limit (per device)
+cudaError_t walk_init_attributes();
 int sort_passes(const DeviceBuffers& b);
 // tree.cu
 void launch_build_fill(const DeviceBuffers& b, int fp64_levels, cudaStream_t s);

@@ -191,6 +191,8 @@ static int validate_config(bh_sim* s, const bh_config& c) {
     if (c.walk_mode == BH_WALK_GROUP && c.bodies_per_lane != 0 && c.bodies_per_lane != 1 &&
         c.bodies_per_lane != 2 && c.bodies_per_lane != 4)
         return fail(s, BH_ERR_INVALID_ARGUMENT, "bodies_per_lane must be 1, 2 or 4");
+    if (c.walk_block != 0 && c.walk_block != 64 && c.walk_block != 128 && c.walk_block != 256)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "walk_block must be 0, 64, 128 or 256");
     if (!(c.far_alpha >= 0.0f && c.far_alpha <= 0.5f))
         return fail(s, BH_ERR_INVALID_ARGUMENT, "far_alpha must be in [0, 0.5]");
     if (!(c.delta_time == c.delta_time) || !(c.bh_theta >= 0.0f))
@@ -645,7 +647,8 @@ static int create_sim(const bh_config* config, const uint32_t* sizes, uint32_t n
         (e = cudaEventCreateWithFlags(&s->ev_copy_order, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&s->ev_mass, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&s->ev_vel, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = bh::sort_init_attributes()) != cudaSuccess) {
+        (e = bh::sort_init_attributes()) != cudaSuccess ||
+        (e = bh::walk_init_attributes()) != cudaSuccess) {
         int r = cuda_fail(nullptr, e, "bh_create");
         delete s;
         return r;
@@ -1359,8 +1362,9 @@ extern "C" int bh_profile_end(bh_sim* s, double* stage_ms, uint32_t* steps_recor
 
 // ---- autotuner (extension) -----------------------------------------------------------
 // Times the group walk on force evaluations at the current positions (which
-// do not advance the state) for every (bodies per lane, leaf size) candidate
-// and keeps the fastest.  The walk's result depends on both (group boxes and
+// do not advance the state) for every (bodies per lane, leaf size) candidate,
+// then the block shape (64, 128 or 256 threads) of the fastest, and keeps
+// the fastest of all.  The walk's result depends on the first two (group boxes and
 // bucket sizes change the interaction lists), so every candidate is a valid
 // configuration with its own accuracy; all stay far inside the group walk's
 // error budget at a given theta.
@@ -1371,6 +1375,7 @@ extern "C" int bh_autotune(bh_sim* s, uint32_t trials, bh_tune_result* out) {
     if (trials == 0) trials = 3;
     static const int kBpl[] = {1, 2, 4};
     static const int kLeaf[] = {2, 4, 8};
+    static const int kBlock[] = {64, 256};  // besides the default 128 of the first sweep
     bh_tune_result best{};
     best.walk_ms = 1e30f;
     cudaEvent_t e0, e1;
@@ -1378,30 +1383,56 @@ extern "C" int bh_autotune(bh_sim* s, uint32_t trials, bh_tune_result* out) {
     BH_CUDA(s, cudaEventCreate(&e1));
     int count = 0;
     const bh_config saved = s->cfg;
+    // Average walk time of the handle's current shape over `trials` launches.
+    auto time_walk = [&](float* out) -> int {
+        float total = 0.f;
+        for (uint32_t t = 0; t <= trials; ++t) {  // trial 0 warms up
+            enqueue_tree(s, [](int) {});
+            cudaEventRecord(e0, s->stream);
+            launch_walk_any(s, walk_params(s, bh::kWalkForces));
+            cudaEventRecord(e1, s->stream);
+            BH_CUDA(s, cudaEventSynchronize(e1));
+            float ms = 0.f;
+            BH_CUDA(s, cudaEventElapsedTime(&ms, e0, e1));
+            if (t > 0) total += ms;
+        }
+        *out = total / (float)trials;
+        return BH_OK;
+    };
+    // Groups and buckets first (block of 128 threads), then the block shape
+    // for the best of them.
     for (int bpl : kBpl) {
         for (int leaf : kLeaf) {
+            if (s->b.n == 0) break;
             s->cfg.bodies_per_lane = bpl;
             s->cfg.leaf_size = leaf;
+            s->cfg.walk_block = 128;
             s->b.group_max = 32u * (uint32_t)bpl;
-            if (s->b.n == 0) break;
-            float total = 0.f;
-            for (uint32_t t = 0; t <= trials; ++t) {  // trial 0 warms up
-                enqueue_tree(s, [](int) {});
-                cudaEventRecord(e0, s->stream);
-                launch_walk_any(s, walk_params(s, bh::kWalkForces));
-                cudaEventRecord(e1, s->stream);
-                BH_CUDA(s, cudaEventSynchronize(e1));
-                float ms = 0.f;
-                BH_CUDA(s, cudaEventElapsedTime(&ms, e0, e1));
-                if (t > 0) total += ms;
-            }
-            const float avg = total / (float)trials;
+            float avg = 0.f;
+            const int rc = time_walk(&avg);
+            if (rc != BH_OK) return rc;
             ++count;
             if (avg < best.walk_ms) {
                 best.walk_ms = avg;
                 best.bodies_per_lane = bpl;
                 best.leaf_size = leaf;
+                best.walk_block = 128;
             }
+        }
+    }
+    for (int block : kBlock) {
+        if (s->b.n == 0) break;
+        s->cfg.bodies_per_lane = best.bodies_per_lane;
+        s->cfg.leaf_size = best.leaf_size;
+        s->cfg.walk_block = block;
+        s->b.group_max = 32u * (uint32_t)best.bodies_per_lane;
+        float avg = 0.f;
+        const int rc = time_walk(&avg);
+        if (rc != BH_OK) return rc;
+        ++count;
+        if (avg < best.walk_ms) {
+            best.walk_ms = avg;
+            best.walk_block = block;
         }
     }
     cudaEventDestroy(e0);
@@ -1410,6 +1441,7 @@ extern "C" int bh_autotune(bh_sim* s, uint32_t trials, bh_tune_result* out) {
     if (count > 0) {
         s->cfg.bodies_per_lane = best.bodies_per_lane;
         s->cfg.leaf_size = best.leaf_size;
+        s->cfg.walk_block = best.walk_block;
     }
     s->b.group_max = 32u * (uint32_t)(s->cfg.bodies_per_lane > 0 ? s->cfg.bodies_per_lane : 2);
     destroy_graphs(s);  // captured steps carry the old walk parameters

@@ -59,7 +59,6 @@
 
 namespace bh {
 
-constexpr int kGroupWarps = 4;
 constexpr int kWalkStack = 384;               // per-warp stack entries
 constexpr int kWalkDfsAt = kWalkStack - 128;  // >= 32 + 96 below the capacity
 
@@ -97,21 +96,28 @@ __device__ __forceinline__ void far_batch(GroupSmem<true>& S, float (&cacc)[kFar
     __syncwarp();
 }
 
-// Resident blocks per SM the register budget is sized for (measured best:
-// 6 for groups of <= 64 bodies; 5 for 128-body groups, whose two packed
-// accumulator pairs per lane need more registers).
-constexpr int walk_min_blocks(int bpl) { return bpl >= 4 ? 5 : 6; }
+// Registers per thread of each variant: the budget of 6 resident 128-thread
+// blocks per SM for groups of <= 64 bodies, 5 for 128-body groups (their two
+// packed accumulator pairs per lane need more; measured best), plus the far
+// field's coefficient sums.  Fixed per variant (not per block size), so the
+// block shape (walk_block: 64, 128 or 256 threads) leaves the warps resident
+// per SM unchanged.
+constexpr int walk_max_regs(int bpl, bool far) {
+    return bpl >= 4 ? (far ? 96 : 80) : (far ? 80 : 72);
+}
 
 // FAR: the far-field variant (Plummer softening, quadrupoles); the other
-// instantiations carry none of its code or registers.
+// instantiations carry none of its code or registers.  Shared memory: one
+// GroupSmem<FAR> per warp, dynamic (the block shape is chosen at launch).
 template <int BPL, int MP, bool PLUMMER, bool FAR>
-__global__ void __launch_bounds__(kGroupWarps * 32, walk_min_blocks(BPL))
+__global__ void __maxnreg__(walk_max_regs(BPL, FAR))
 walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ node4,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ ids,
                   float2* __restrict__ pos, float2* __restrict__ vel, float2* __restrict__ acc,
                   const WalkParams P, uint32_t* __restrict__ err) {
     constexpr int NP = BPL / 2;  // packed pairs per lane (BPL >= 2)
-    __shared__ GroupSmem<FAR> smem[kGroupWarps];
+    extern __shared__ __align__(16) unsigned char walk_smem[];
+    GroupSmem<FAR>* smem = reinterpret_cast<GroupSmem<FAR>*>(walk_smem);
     if (step_failed(err)) return;  // the tree of this step was not built
     const int lane = threadIdx.x & 31;
     GroupSmem<FAR>& S = smem[threadIdx.x >> 5];
@@ -526,46 +532,82 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
     }
 }
 
+// Warps per block the group walk may run with (walk_block / 32).
+constexpr int kWalkShapes[3] = {2, 4, 8};
+constexpr int kWalkDefaultWarps = 4;
+
+static int shape_index(int warps) { return warps == 2 ? 0 : (warps == 8 ? 2 : 1); }
+
+template <int BPL, int MP, bool PL, bool FAR>
+static cudaError_t set_walk_attributes() {
+    return cudaFuncSetAttribute(walk_group_kernel<BPL, MP, PL, FAR>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(8 * sizeof(GroupSmem<FAR>)));
+}
+
 template <int BPL, int MP, bool PL, bool FAR = false>
-static void launch_t(const DeviceBuffers& b, const WalkParams& p, cudaStream_t s) {
-    static int blocks_per_sm[64] = {};
+static void launch_t(const DeviceBuffers& b, const WalkParams& p, int warps, cudaStream_t s) {
+    static int blocks_per_sm[64][3] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    int& bps = blocks_per_sm[dev & 63];
+    const size_t smem = (size_t)warps * sizeof(GroupSmem<FAR>);
+    int& bps = blocks_per_sm[dev & 63][shape_index(warps)];
     if (bps == 0) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, walk_group_kernel<BPL, MP, PL, FAR>,
-                                                      kGroupWarps * 32, 0);
+                                                      warps * 32, smem);
         if (bps < 1) bps = 1;
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     // Persistent grid; the number of groups (<= n) is only known on the device.
     uint32_t blocks = (uint32_t)(sms * bps);
-    const uint32_t need = (b.n + kGroupWarps - 1) / kGroupWarps;
+    const uint32_t need = (b.n + warps - 1) / warps;
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
-    walk_group_kernel<BPL, MP, PL, FAR><<<blocks, kGroupWarps * 32, 0, s>>>(
+    walk_group_kernel<BPL, MP, PL, FAR><<<blocks, warps * 32, smem, s>>>(
         b.gnode, b.node4, b.groups, b.ids, b.pos, b.vel, b.acc, p, b.err);
 }
 
 template <int BPL>
-static void launch_bpl(const DeviceBuffers& b, const WalkParams& p, cudaStream_t s) {
+static void launch_bpl(const DeviceBuffers& b, const WalkParams& p, int warps, cudaStream_t s) {
     if (p.multipole >= 2) {
-        if (p.plummer && p.far_alpha2 > 0.0f) launch_t<BPL, 2, true, true>(b, p, s);
-        else if (p.plummer) launch_t<BPL, 2, true>(b, p, s);
-        else launch_t<BPL, 2, false>(b, p, s);
+        if (p.plummer && p.far_alpha2 > 0.0f) launch_t<BPL, 2, true, true>(b, p, warps, s);
+        else if (p.plummer) launch_t<BPL, 2, true>(b, p, warps, s);
+        else launch_t<BPL, 2, false>(b, p, warps, s);
     } else {
-        if (p.plummer) launch_t<BPL, 1, true>(b, p, s); else launch_t<BPL, 1, false>(b, p, s);
+        if (p.plummer) launch_t<BPL, 1, true>(b, p, warps, s);
+        else launch_t<BPL, 1, false>(b, p, warps, s);
     }
 }
 
+template <int BPL>
+static cudaError_t set_bpl_attributes() {
+    cudaError_t e;
+    if ((e = set_walk_attributes<BPL, 2, true, true>()) != cudaSuccess) return e;
+    if ((e = set_walk_attributes<BPL, 2, true, false>()) != cudaSuccess) return e;
+    if ((e = set_walk_attributes<BPL, 2, false, false>()) != cudaSuccess) return e;
+    if ((e = set_walk_attributes<BPL, 1, true, false>()) != cudaSuccess) return e;
+    return set_walk_attributes<BPL, 1, false, false>();
+}
+
+// Allow every walk variant the dynamic shared memory of its largest block
+// shape on the current device (once per device, before any launch or
+// capture).
+cudaError_t walk_init_attributes() {
+    cudaError_t e;
+    if ((e = set_bpl_attributes<1>()) != cudaSuccess) return e;
+    if ((e = set_bpl_attributes<2>()) != cudaSuccess) return e;
+    return set_bpl_attributes<4>();
+}
+
 void launch_walk_group(const DeviceBuffers& b, const WalkParams& p, int block, cudaStream_t s) {
-    (void)block;
     if (b.n == 0) return;
+    int warps = block / 32;
+    if (warps != 2 && warps != 4 && warps != 8) warps = kWalkDefaultWarps;
     switch (p.bpl) {
-        case 1: launch_bpl<1>(b, p, s); break;
-        case 4: launch_bpl<4>(b, p, s); break;
-        default: launch_bpl<2>(b, p, s); break;
+        case 1: launch_bpl<1>(b, p, warps, s); break;
+        case 4: launch_bpl<4>(b, p, warps, s); break;
+        default: launch_bpl<2>(b, p, warps, s); break;
     }
 }
 

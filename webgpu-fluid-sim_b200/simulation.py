@@ -220,13 +220,13 @@ class Simulation:
         return {k: float(ms[i]) for i, k in enumerate(_lib.BH_STAGE_NAMES)}, int(cnt.value)
 
     def autotune(self, trials: int = 3) -> dict:
-        """Pick the fastest (bodies per lane, leaf size) for the group walk."""
+        """Pick the fastest (bodies per lane, leaf size, walk block) for the group walk."""
         r = _lib.bh_tune_result()
         self._check(self._lib.bh_autotune(self._h, int(trials), ctypes.byref(r)))
         self.config = dataclasses.replace(self.config, bodiesPerLane=r.bodies_per_lane,
-                                          leafSize=r.leaf_size)
+                                          leafSize=r.leaf_size, walkBlock=r.walk_block)
         return {"bodiesPerLane": r.bodies_per_lane, "leafSize": r.leaf_size,
-                "walk_ms": r.walk_ms, "candidates": r.candidates}
+                "walkBlock": r.walk_block, "walk_ms": r.walk_ms, "candidates": r.candidates}
 
     def force_vjp(self, abar) -> tuple[np.ndarray, np.ndarray]:
         """(da/dx)^T abar and (da/dm)^T abar at the current positions."""
