@@ -86,9 +86,11 @@ def test_rollout_gradient_matches_fp64_adjoint_4096(bh, orc):
     Lr, rx, rv, rm = orc.rollout_grad_fp64(orc.params_from_config(sim.config), mass, pos, vel, tgt,
                                           steps)
     assert abs(L - Lr) <= 1e-2 * Lr
-    for g, r in ((gx, rx), (gv, rv), (gm, rm)):
-        assert np.linalg.norm(g - r) <= 5e-2 * np.linalg.norm(r)
+    for name, g, r in (("x0", gx, rx), ("v0", gv, rv), ("m", gm, rm)):
+        rel = float(np.linalg.norm(g - r) / np.linalg.norm(r))
         cos = float((g * r).sum() / (np.linalg.norm(g) * np.linalg.norm(r)))
+        print(f"rollout gradient d/d{name} vs FP64 adjoint: relative error {rel:.3e}, cosine {cos:.6f}")
+        assert rel <= 5e-2
         assert cos > 0.995
     # the handle is left at step T
     _, p_end, _ = sim.download()
@@ -124,5 +126,7 @@ def test_rollout_gradient_matches_finite_differences(bh):
         fd = (loss(*args(plus)) - loss(*args(minus))) / (2 * h)
         g = {"x": gx, "v": gv, "m": gm}[which]
         ad = float((g.astype(np.float64) * d).sum())
+        print(f"directional derivative along d{which}: adjoint {ad:.6e}, central FD {fd:.6e}, "
+              f"relative difference {abs(fd - ad) / abs(ad):.3e}")
         assert abs(fd - ad) <= 5e-2 * abs(ad) + 1e-9, (which, fd, ad)
     sim.close()

@@ -29,12 +29,6 @@ constexpr int kSortItems = BH_SORT_ITEMS;
 constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 256;
-// 1: the sort's last pass writes the leaf records (gathering each sorted
-// slot's packed body record with several loads in flight per thread), so
-// the hierarchy build reads them in slot order; 0: the build gathers them.
-#ifndef BH_LEAVES_IN_SORT
-#define BH_LEAVES_IN_SORT 1
-#endif
 
 // Device error word bits (read by the host after a sync).
 constexpr uint32_t kErrLookbackSpin = 1u << 0;  // decoupled look-back gave up waiting
@@ -160,9 +154,6 @@ struct DeviceBuffers {
     float2* acc = nullptr;
     float* radius = nullptr;
     float4* xm = nullptr;   // {x, y, m, 0} per body (original order), written by the encode
-    // the sort's last pass writes the leaf records from xm (else the build
-    // gathers them itself)
-    bool leaves_in_sort = BH_LEAVES_IN_SORT != 0;
     // sort
     void* codes = nullptr;      // sorted keys after a step
     void* codes_alt = nullptr;

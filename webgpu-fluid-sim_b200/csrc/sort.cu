@@ -67,8 +67,7 @@ __global__ void __launch_bounds__(kSortThreads, BH_SORT_MIN_BLOCKS)
 onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_in,
                 K* __restrict__ keys_out, uint32_t* __restrict__ ids_out, uint32_t n, int pass,
                 StepScratch* __restrict__ scratch, uint32_t* __restrict__ status, uint32_t tiles,
-                uint32_t* __restrict__ err, uint32_t spin_cap, uint32_t debug_flags,
-                const float4* __restrict__ xm, float4* __restrict__ leaves) {
+                uint32_t* __restrict__ err, uint32_t spin_cap, uint32_t debug_flags) {
     constexpr int W = kSortThreads / 32;
     __shared__ uint32_t s_whist[W][kRadix];
     __shared__ uint32_t s_tile_excl[kRadix];
@@ -215,54 +214,16 @@ onesweep_kernel(const K* __restrict__ keys_in, const uint32_t* __restrict__ ids_
     __syncthreads();
     const uint32_t tile_base = tile * kSortTile;
     const uint32_t tile_n = (n - tile_base) < (uint32_t)kSortTile ? (n - tile_base) : (uint32_t)kSortTile;
-    if (leaves == nullptr) {
-        for (uint32_t i = (uint32_t)tid; i < tile_n; i += kSortThreads) {
-            K kk = s_keys[i];
-            uint32_t dd = (uint32_t)(kk >> shift) & 0xFFu;
-            uint32_t dst = s_gbase[dd] + (i - s_tile_excl[dd]);
-            // Offsets are in range unless a look-back gave up; never write outside.
-            if (dst < n) {
-                keys_out[dst] = kk;
-                ids_out[dst] = s_ids[i];
-            } else {
-                atomicOr(err, kErrLookbackSpin);
-            }
-        }
-        return;
-    }
-    // Last pass: also the leaf record of each sorted slot, gathered from the
-    // body's packed record -- kLeafBatch independent gathers per thread in
-    // flight, so the hierarchy build reads its leaves in slot order.
-    constexpr int kLeafBatch = 4;
-    for (uint32_t i0 = (uint32_t)tid; i0 < tile_n; i0 += kLeafBatch * kSortThreads) {
-        uint32_t dst[kLeafBatch], id[kLeafBatch];
-        float4 rec[kLeafBatch];
-#pragma unroll
-        for (int k = 0; k < kLeafBatch; ++k) {
-            const uint32_t i = i0 + (uint32_t)k * kSortThreads;
-            dst[k] = n;
-            id[k] = 0;
-            if (i < tile_n) {
-                const K kk = s_keys[i];
-                const uint32_t dd = (uint32_t)(kk >> shift) & 0xFFu;
-                dst[k] = s_gbase[dd] + (i - s_tile_excl[dd]);
-                id[k] = s_ids[i];
-                if (dst[k] < n) keys_out[dst[k]] = kk;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kLeafBatch; ++k)
-            if (dst[k] < n && id[k] < n) rec[k] = __ldg(&xm[id[k]]);
-#pragma unroll
-        for (int k = 0; k < kLeafBatch; ++k) {
-            const uint32_t i = i0 + (uint32_t)k * kSortThreads;
-            if (i >= tile_n) continue;
-            if (dst[k] < n && id[k] < n) {
-                ids_out[dst[k]] = id[k];
-                leaves[dst[k]] = rec[k];
-            } else {
-                atomicOr(err, kErrLookbackSpin);
-            }
+    for (uint32_t i = (uint32_t)tid; i < tile_n; i += kSortThreads) {
+        K kk = s_keys[i];
+        uint32_t dd = (uint32_t)(kk >> shift) & 0xFFu;
+        uint32_t dst = s_gbase[dd] + (i - s_tile_excl[dd]);
+        // Offsets are in range unless a look-back gave up; never write outside.
+        if (dst < n) {
+            keys_out[dst] = kk;
+            ids_out[dst] = s_ids[i];
+        } else {
+            atomicOr(err, kErrLookbackSpin);
         }
     }
 }
@@ -279,19 +240,15 @@ static void sort_impl(const DeviceBuffers& b, cudaStream_t s) {
     K* kout = (K*)b.codes_alt;
     uint32_t* iin = b.ids;
     uint32_t* iout = b.ids_alt;
-    // With packed body records from the encode, the last pass also writes
-    // every sorted slot's leaf record (node4[n - 1 + slot]).
-    float4* leaves = (b.xm && b.leaves_in_sort) ? b.node4 + (b.n - 1) : nullptr;
     for (int p = 0; p < passes; ++p) {
-        float4* lv = (p == passes - 1) ? leaves : nullptr;
         if (p == 0)
             onesweep_kernel<K, true><<<b.tiles, kSortThreads, smem, s>>>(
                 kin, nullptr, kout, iout, b.n, p, b.scratch, b.status, b.tiles, b.err, b.spin_cap,
-                b.debug_flags, b.xm, lv);
+                b.debug_flags);
         else
             onesweep_kernel<K, false><<<b.tiles, kSortThreads, smem, s>>>(
                 kin, iin, kout, iout, b.n, p, b.scratch, b.status, b.tiles, b.err, b.spin_cap,
-                b.debug_flags, b.xm, lv);
+                b.debug_flags);
         K* tk = kin; kin = kout; kout = tk;
         uint32_t* ti = iin; iin = iout; iout = ti;
     }

@@ -33,7 +33,6 @@ static void launch_typed(const DeviceBuffers& b, int fp64_levels, cudaStream_t s
     a.group_count = b.groups ? &b.scratch->group_ctr[1] : nullptr;
     a.gmax = b.group_max;
     a.xm = b.xm;
-    a.leaves_ready = b.xm != nullptr && b.leaves_in_sort;
     a.err = b.err;
     if (!split_build(b.n)) {
         constexpr uint32_t B = build_block<false>();

@@ -97,9 +97,6 @@ struct BuildArgs {
     // {x, y, m, 0} per body in original order, when the encode wrote them:
     // one gather per slot instead of a position and a mass
     const float4* xm = nullptr;
-    // The sort's last pass already wrote every leaf record node4[n-1+slot]
-    // (from xm): the build reads them in slot order.
-    bool leaves_ready = false;
     // The step's device error word: when an earlier stage of the step failed
     // (kErrSkipMask), the build does nothing.  Null: no such check.
     const uint32_t* err = nullptr;
@@ -443,25 +440,18 @@ build_fill_kernel(const BuildArgs<K> A) {
     }
     if (i >= n) return;
 
+    const uint32_t body = __ldg(&A.ids[i]);
     float m;
     float2 p;
-    if (A.leaves_ready) {
-        // written by the sort's last pass (lbvh.wgsl:179-187)
-        const float4 r = __ldcg(&A.node4[nm1 + i]);
+    if (A.xm) {
+        const float4 r = __ldg(&A.xm[body]);
         m = r.z;
         p = make_float2(r.x, r.y);
     } else {
-        const uint32_t body = __ldg(&A.ids[i]);
-        if (A.xm) {
-            const float4 r = __ldg(&A.xm[body]);
-            m = r.z;
-            p = make_float2(r.x, r.y);
-        } else {
-            m = __ldg(&A.mass[body]);
-            p = __ldg(&A.pos[body]);
-        }
-        A.node4[nm1 + i] = make_float4(p.x, p.y, m, 0.0f);  // leaf (lbvh.wgsl:179-187)
+        m = __ldg(&A.mass[body]);
+        p = __ldg(&A.pos[body]);
     }
+    A.node4[nm1 + i] = make_float4(p.x, p.y, m, 0.0f);  // leaf (lbvh.wgsl:179-187)
     S.leaf[0][t] = m;
     S.leaf[1][t] = p.x;
     S.leaf[2][t] = p.y;

@@ -96,21 +96,22 @@ __device__ __forceinline__ void far_batch(GroupSmem<true>& S, float (&cacc)[kFar
     __syncwarp();
 }
 
-// Registers per thread of each variant: the budget of 6 resident 128-thread
-// blocks per SM for groups of <= 64 bodies, 5 for 128-body groups (their two
-// packed accumulator pairs per lane need more; measured best), plus the far
-// field's coefficient sums.  Fixed per variant (not per block size), so the
-// block shape (walk_block: 64, 128 or 256 threads) leaves the warps resident
-// per SM unchanged.
-constexpr int walk_max_regs(int bpl, bool far) {
-    return bpl >= 4 ? (far ? 96 : 80) : (far ? 80 : 72);
-}
+// Register budget: launch bounds for blocks of up to 256 threads with 3
+// resident per SM for groups of <= 64 bodies (at most 85 registers, the
+// budget of 6 resident 128-thread blocks), 2 for 128-body groups, whose two
+// packed accumulator pairs per lane need more.  The bound is the same for
+// every block shape (walk_block: 64, 128 or 256 threads), so the shape leaves
+// the warps resident per SM unchanged.  (An explicit register cap of 72 in
+// place of these bounds gave a 65-register build of the 64-body walk that
+// ran 12% slower.)
+constexpr int kWalkMaxThreads = 256;
+constexpr int walk_min_blocks(int bpl) { return bpl >= 4 ? 2 : 3; }
 
 // FAR: the far-field variant (Plummer softening, quadrupoles); the other
 // instantiations carry none of its code or registers.  Shared memory: one
 // GroupSmem<FAR> per warp, dynamic (the block shape is chosen at launch).
 template <int BPL, int MP, bool PLUMMER, bool FAR>
-__global__ void __maxnreg__(walk_max_regs(BPL, FAR))
+__global__ void __launch_bounds__(kWalkMaxThreads, walk_min_blocks(BPL))
 walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ node4,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ ids,
                   float2* __restrict__ pos, float2* __restrict__ vel, float2* __restrict__ acc,
