@@ -67,10 +67,10 @@ STREAM_BYTES = {4: {"morton": 8 + 4 + 4 + 16, "sort": 12 + 3 * 16, "tree": 4 + 4
 # the engine package: body count, scenario and the oracle's parameters
 # (oracle.params keywords).  tests/test_bench.py checks them against the
 # package's WORKLOADS.
-def _orc_params(theta, eps, dt, bits, domain, integrator):
+def _orc_params(theta, eps, dt, bits, domain, integrator, far_alpha=0.0):
     return dict(G=1.0, dt=dt, theta=theta, softening="plummer", plummer_eps=eps,
                 morton_bits=bits, morton_domain=domain, integrator=integrator, leaf_size=8,
-                walk="group", multipole=2, bodies_per_lane=2)
+                walk="group", multipole=2, bodies_per_lane=2, far_alpha=far_alpha)
 
 
 REF_WORKLOADS = {
@@ -78,13 +78,13 @@ REF_WORKLOADS = {
                              oracle=_orc_params(0.7, 1e-3, 1e-4, 32, "bbox", "leapfrog-kdk")),
     "colliding-disks-800k": dict(n=800_000, scenario="colliding-disks",
                                  oracle=_orc_params(0.5, 1e-3, 5e-5, 32, "bbox",
-                                                    "symplectic-euler")),
+                                                    "symplectic-euler", 0.4)),
     "gaussian-mixture-16m": dict(n=16_777_216, scenario="gaussian-mixture",
                                  oracle=_orc_params(0.5, 1e-4, 1e-5, 64, "fixed2000",
-                                                    "symplectic-euler")),
+                                                    "symplectic-euler", 0.4)),
     "gaussian-mixture-4m": dict(n=4_194_304, scenario="gaussian-mixture",
                                 oracle=_orc_params(0.5, 1e-4, 1e-5, 64, "fixed2000",
-                                                   "symplectic-euler")),
+                                                   "symplectic-euler", 0.4)),
 }
 
 
@@ -332,7 +332,8 @@ def ensemble_cost(pkg, device: int, systems: int = 1024, steps: int = 100,
     `loop_steps` steps."""
     import torch
     cfg = pkg.Config(bhTheta=0.5, deltaTime=1e-4, softening="plummer", plummerEps=1e-3,
-                     mortonDomain="bbox", integrator="leapfrog-kdk", walk="group", leafSize=8)
+                     mortonDomain="bbox", integrator="leapfrog-kdk", walk="group", leafSize=8,
+                     farAlpha=pkg.config.FAR_ALPHA)
     sizes = pkg.ensemble_sizes(systems, 2024, 1024, 262144)
     total = int(sizes.sum())
     dev = torch.device("cuda", device)

@@ -24,9 +24,10 @@ def test_reference_workloads_match_the_package(bh):
         op = wp["oracle"]
         got = (op["G"], op["dt"], op["theta"], op["softening"], op["plummer_eps"],
                op["morton_bits"], op["morton_domain"], op["integrator"], op["walk"],
-               op["multipole"])
+               op["multipole"], op["far_alpha"])
         want = (cfg.gravConstant, cfg.deltaTime, cfg.bhTheta, cfg.softening, cfg.plummerEps,
-                cfg.mortonBits, cfg.mortonDomain, cfg.integrator, cfg.walk, cfg.multipole)
+                cfg.mortonBits, cfg.mortonDomain, cfg.integrator, cfg.walk, cfg.multipole,
+                cfg.farAlpha)
         assert got == want, name
 
 
