@@ -15,7 +15,10 @@ namespace bh {
 constexpr uint32_t kSentinel = 0xFFFFFFFFu;
 constexpr int kStackSize = 256;  // barnes_hut.wgsl:67
 // Nodes with at least this many bodies aggregate mass/COM in FP64.
-constexpr uint32_t kFp64MinBodies = 1024;
+#ifndef BH_FP64_MIN_BODIES
+#define BH_FP64_MIN_BODIES 1024
+#endif
+constexpr uint32_t kFp64MinBodies = BH_FP64_MIN_BODIES;
 
 // Sort tiling (a tile is kSortThreads x kSortItems keys).
 #ifndef BH_SORT_THREADS
@@ -213,6 +216,8 @@ void launch_sort(const DeviceBuffers& b, cudaStream_t s);
 cudaError_t sort_init_attributes();
 // walk_group.cu: the group walk's dynamic shared memory limit (per device)
 cudaError_t walk_init_attributes();
+// tree.cu: the hierarchy build's dynamic shared memory limit (per device)
+cudaError_t build_init_attributes();
 int sort_passes(const DeviceBuffers& b);
 // tree.cu
 void launch_build_fill(const DeviceBuffers& b, int fp64_levels, cudaStream_t s);

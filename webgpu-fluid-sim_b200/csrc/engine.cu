@@ -648,7 +648,8 @@ static int create_sim(const bh_config* config, const uint32_t* sizes, uint32_t n
         (e = cudaEventCreateWithFlags(&s->ev_mass, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&s->ev_vel, cudaEventDisableTiming)) != cudaSuccess ||
         (e = bh::sort_init_attributes()) != cudaSuccess ||
-        (e = bh::walk_init_attributes()) != cudaSuccess) {
+        (e = bh::walk_init_attributes()) != cudaSuccess ||
+        (e = bh::build_init_attributes()) != cudaSuccess) {
         int r = cuda_fail(nullptr, e, "bh_create");
         delete s;
         return r;

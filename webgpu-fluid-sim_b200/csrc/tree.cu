@@ -8,6 +8,23 @@ namespace bh {
 
 bool split_build(uint32_t n) { return n >= kSplitBuildMin; }
 
+template <typename K, bool SPLIT>
+static cudaError_t set_build_attributes() {
+    return cudaFuncSetAttribute(build_fill_kernel<K, SPLIT>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(BuildShared<K, build_block<SPLIT>()>));
+}
+
+// Allow the build kernels their shared memory (dynamic; once per device,
+// before any launch or capture).
+cudaError_t build_init_attributes() {
+    cudaError_t e;
+    if ((e = set_build_attributes<uint32_t, false>()) != cudaSuccess) return e;
+    if ((e = set_build_attributes<uint32_t, true>()) != cudaSuccess) return e;
+    if ((e = set_build_attributes<uint64_t, false>()) != cudaSuccess) return e;
+    return set_build_attributes<uint64_t, true>();
+}
+
 void init_bound(const DeviceBuffers& b, cudaStream_t s) {
     if (b.n > 1) cudaMemsetAsync(b.bound, 0xFF, sizeof(uint32_t) * (b.n - 1), s);
 }
@@ -36,14 +53,14 @@ static void launch_typed(const DeviceBuffers& b, int fp64_levels, cudaStream_t s
     a.err = b.err;
     if (!split_build(b.n)) {
         constexpr uint32_t B = build_block<false>();
-        build_fill_kernel<K, false><<<(b.n + B - 1) / B, B, 0, s>>>(a);
+        build_fill_kernel<K, false><<<(b.n + B - 1) / B, B, sizeof(BuildShared<K, B>), s>>>(a);
         return;
     }
     a.frontier = b.frontier;
     a.frontier_count = &b.scratch->frontier_ctr;
     constexpr uint32_t B = build_block<true>();
     const uint32_t grid = (b.n + B - 1) / B;
-    build_fill_kernel<K, true><<<grid, B, 0, s>>>(a);
+    build_fill_kernel<K, true><<<grid, B, sizeof(BuildShared<K, B>), s>>>(a);
     // Frontier nodes number far fewer than bodies (a handful per CTA), but
     // only the device knows how many: a resident grid strides over them.
     static int blocks_per_sm[64] = {};

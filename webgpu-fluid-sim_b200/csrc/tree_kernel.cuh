@@ -110,8 +110,14 @@ struct BuildArgs {
 // (800k bodies: 128 -> 0.137 ms, 256 -> 0.140, 512 -> 0.150), the local phase
 // of the split build with large ones (16.8M: 128 -> 2.11 ms, 256 -> 1.83,
 // 512 -> 1.72).  The frontier climb keeps 256 threads per CTA.
-constexpr int kBuildBlockFused = 128;
-constexpr int kBuildBlockSplit = 512;
+#ifndef BH_BUILD_BLOCK_FUSED
+#define BH_BUILD_BLOCK_FUSED 128
+#endif
+#ifndef BH_BUILD_BLOCK_SPLIT
+#define BH_BUILD_BLOCK_SPLIT 512
+#endif
+constexpr int kBuildBlockFused = BH_BUILD_BLOCK_FUSED;
+constexpr int kBuildBlockSplit = BH_BUILD_BLOCK_SPLIT;
 constexpr int kClimbBlock = 256;
 template <bool SPLIT>
 constexpr int build_block() { return SPLIT ? kBuildBlockSplit : kBuildBlockFused; }
@@ -373,7 +379,9 @@ template <typename K, bool SPLIT>
 __global__ void __launch_bounds__(build_block<SPLIT>())
 build_fill_kernel(const BuildArgs<K> A) {
     constexpr int B = build_block<SPLIT>();
-    __shared__ BuildShared<K, B> S;
+    // dynamic: sizeof(BuildShared<K, B>) bytes (more than 48 KB for large B)
+    extern __shared__ __align__(16) unsigned char build_smem[];
+    BuildShared<K, B>& S = *reinterpret_cast<BuildShared<K, B>*>(build_smem);
 
     const uint32_t n = A.n;
     if (step_failed(A.err)) return;  // uniform over the block

@@ -81,7 +81,7 @@ static void launch_static(const void* codes, const uint32_t* ids, const float* m
     a.group_count = nullptr;
     a.gmax = 0u;
     constexpr uint32_t B = build_block<false>();
-    build_fill_kernel<K, false><<<(n + B - 1) / B, B, 0, s>>>(a);
+    build_fill_kernel<K, false><<<(n + B - 1) / B, B, sizeof(BuildShared<K, B>), s>>>(a);
 }
 
 }  // namespace bh
