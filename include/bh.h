@@ -228,9 +228,9 @@ typedef struct bh_tune_result {
 /* Time the group walk (on force evaluations at the current positions, which
  * do not advance the state) for bodies_per_lane in {1, 2, 4} x leaf_size in
  * {2, 4, 8} with 128-thread blocks, then the best of those with 64- and
- * 256-thread blocks (walk_block), `trials` launches each after one warm-up,
- * and keep the fastest in the handle's configuration (11 candidates).
- * Group walk only. */
+ * 256-thread blocks (walk_block; 128-body groups run blocks of at most 128
+ * threads), `trials` launches each after one warm-up, and keep the fastest
+ * in the handle's configuration (10 or 11 candidates).  Group walk only. */
 int bh_autotune(bh_sim* sim, uint32_t trials, bh_tune_result* out);
 
 /* The handle's current configuration (after bh_autotune, for instance). */

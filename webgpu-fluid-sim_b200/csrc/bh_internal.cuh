@@ -214,8 +214,10 @@ void launch_encode_ensemble(const DeviceBuffers& b, cudaStream_t s);
 void launch_zero_step(const DeviceBuffers& b, cudaStream_t s);  // scratch + sort status
 void launch_sort(const DeviceBuffers& b, cudaStream_t s);
 cudaError_t sort_init_attributes();
-// walk_group.cu: the group walk's dynamic shared memory limit (per device)
+// walk_group.cu: the group walk's dynamic shared memory limit (per device),
+// and its largest block (threads) for a bodies_per_lane
 cudaError_t walk_init_attributes();
+int walk_group_max_block(int bpl);
 // tree.cu: the hierarchy build's dynamic shared memory limit (per device)
 cudaError_t build_init_attributes();
 int sort_passes(const DeviceBuffers& b);

@@ -1423,6 +1423,7 @@ extern "C" int bh_autotune(bh_sim* s, uint32_t trials, bh_tune_result* out) {
     }
     for (int block : kBlock) {
         if (s->b.n == 0) break;
+        if (block > bh::walk_group_max_block(best.bodies_per_lane)) continue;
         s->cfg.bodies_per_lane = best.bodies_per_lane;
         s->cfg.leaf_size = best.leaf_size;
         s->cfg.walk_block = block;

@@ -98,20 +98,24 @@ __device__ __forceinline__ void far_batch(GroupSmem<true>& S, float (&cacc)[kFar
 
 // Register budget: launch bounds for blocks of up to 256 threads with 3
 // resident per SM for groups of <= 64 bodies (at most 85 registers, the
-// budget of 6 resident 128-thread blocks), 2 for 128-body groups, whose two
-// packed accumulator pairs per lane need more.  The bound is the same for
-// every block shape (walk_block: 64, 128 or 256 threads), so the shape leaves
-// the warps resident per SM unchanged.  (An explicit register cap of 72 in
-// place of these bounds gave a 65-register build of the 64-body walk that
-// ran 12% slower.)
-constexpr int kWalkMaxThreads = 256;
-constexpr int walk_min_blocks(int bpl) { return bpl >= 4 ? 2 : 3; }
+// budget of 6 resident 128-thread blocks); for 128-body groups, whose two
+// packed accumulator pairs per lane need more, blocks of up to 128 threads
+// with 5 resident (at most 102).  The bound does not depend on the block
+// shape chosen at launch (walk_block: 64, 128 or, for groups of <= 64
+// bodies, 256 threads), so the shape leaves the warps resident per SM
+// unchanged.  (An explicit register cap of 72 in place of these bounds gave
+// a 65-register build of the 64-body walk that ran 12% slower.)
+constexpr int walk_max_threads(int bpl) { return bpl >= 4 ? 128 : 256; }
+#ifndef BH_WALK_MIN_BLOCKS_128
+#define BH_WALK_MIN_BLOCKS_128 5
+#endif
+constexpr int walk_min_blocks(int bpl) { return bpl >= 4 ? BH_WALK_MIN_BLOCKS_128 : 3; }
 
 // FAR: the far-field variant (Plummer softening, quadrupoles); the other
 // instantiations carry none of its code or registers.  Shared memory: one
 // GroupSmem<FAR> per warp, dynamic (the block shape is chosen at launch).
 template <int BPL, int MP, bool PLUMMER, bool FAR>
-__global__ void __launch_bounds__(kWalkMaxThreads, walk_min_blocks(BPL))
+__global__ void __launch_bounds__(walk_max_threads(BPL), walk_min_blocks(BPL))
 walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ node4,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ ids,
                   float2* __restrict__ pos, float2* __restrict__ vel, float2* __restrict__ acc,
@@ -418,39 +422,29 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
             }
             if (counting) c_vis += (unsigned long long)k;
             __syncwarp();
-            if (nn >= 32) {
+            // Lists are evaluated when full, and whatever they hold once the
+            // stack is empty; one call site each keeps the kernel's code
+            // (and its instruction-cache footprint) small.
+            const bool last = sp == 0;
+            if (nn >= 32 || (last && nn > 0)) {
                 eval_nodes(nn);
                 if (counting) c_node += (unsigned long long)nn * nvalid;
                 nn = 0;
                 __syncwarp();
             }
-            if (ns >= 32) {
+            if (ns >= 32 || (last && ns > 0)) {
                 if (counting) c_body += (unsigned long long)ns * nvalid;
                 eval_bodies(ns);
                 ns = 0;
             }
             if constexpr (FAR) {
-                if (nf >= 32) {
-                    far_batch(S, cacc, lane, nf, 32, gcx, gcy, lam, eps2);
-                    if (counting) c_far += 32ull;
-                    nf -= 32;
+                while (nf >= 32 || (last && nf > 0)) {
+                    const int cnt = nf < 32 ? nf : 32;
+                    far_batch(S, cacc, lane, nf, cnt, gcx, gcy, lam, eps2);
+                    if (counting) c_far += (unsigned long long)cnt;
+                    nf -= cnt;
                     far_used = true;
                 }
-            }
-        }
-        if (nn > 0) {
-            eval_nodes(nn);
-            if (counting) c_node += (unsigned long long)nn * nvalid;
-        }
-        if (ns > 0) {
-            if (counting) c_body += (unsigned long long)ns * nvalid;
-            eval_bodies(ns);
-        }
-        if constexpr (FAR) {
-            if (nf > 0) {
-                far_batch(S, cacc, lane, nf, nf, gcx, gcy, lam, eps2);
-                if (counting) c_far += (unsigned long long)nf;
-                far_used = true;
             }
         }
         if (counting && n > 1) c_body -= nvalid;  // each body met its own leaf once
@@ -543,8 +537,11 @@ template <int BPL, int MP, bool PL, bool FAR>
 static cudaError_t set_walk_attributes() {
     return cudaFuncSetAttribute(walk_group_kernel<BPL, MP, PL, FAR>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(8 * sizeof(GroupSmem<FAR>)));
+                                (int)(walk_max_threads(BPL) / 32 * sizeof(GroupSmem<FAR>)));
 }
+
+// Largest walk block for bodies_per_lane `bpl` (its launch bound).
+int walk_group_max_block(int bpl) { return walk_max_threads(bpl >= 4 ? 4 : 2); }
 
 template <int BPL, int MP, bool PL, bool FAR = false>
 static void launch_t(const DeviceBuffers& b, const WalkParams& p, int warps, cudaStream_t s) {
@@ -605,6 +602,7 @@ void launch_walk_group(const DeviceBuffers& b, const WalkParams& p, int block, c
     if (b.n == 0) return;
     int warps = block / 32;
     if (warps != 2 && warps != 4 && warps != 8) warps = kWalkDefaultWarps;
+    if (warps * 32 > walk_group_max_block(p.bpl)) warps = walk_group_max_block(p.bpl) / 32;
     switch (p.bpl) {
         case 1: launch_bpl<1>(b, p, warps, s); break;
         case 4: launch_bpl<4>(b, p, warps, s); break;
