@@ -80,6 +80,7 @@ struct bh_sim {
     // ensemble of independent systems (empty: one system)
     std::vector<uint32_t> sys_sizes;
     std::string err;
+    uint32_t* err_host = nullptr;  // page-locked copy of the device error word
 };
 
 static thread_local std::string g_err;
@@ -542,10 +543,13 @@ static cudaEvent_t* prof_slot(bh_sim* s) {
     return &s->prof_ev[(size_t)s->prof_used * kMarkers];
 }
 
+// Synchronises the handle's stream once, after the work the caller enqueued
+// and a copy of the device error word into page-locked host memory.
 static int check_device_errors(bh_sim* s) {
-    uint32_t e = 0;
-    BH_CUDA(s, cudaMemcpyAsync(&e, s->b.err, sizeof(e), cudaMemcpyDeviceToHost, s->stream));
+    BH_CUDA(s, cudaMemcpyAsync(s->err_host, s->b.err, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                               s->stream));
     BH_CUDA(s, cudaStreamSynchronize(s->stream));
+    const uint32_t e = *s->err_host;
     if (e == 0) return BH_OK;
     BH_CUDA(s, cudaMemsetAsync(s->b.err, 0, sizeof(uint32_t), s->stream));
     std::string msg = "device check failed:";
@@ -647,6 +651,7 @@ static int create_sim(const bh_config* config, const uint32_t* sizes, uint32_t n
         (e = cudaEventCreateWithFlags(&s->ev_copy_order, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&s->ev_mass, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&s->ev_vel, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaHostAlloc((void**)&s->err_host, sizeof(uint32_t), cudaHostAllocDefault)) != cudaSuccess ||
         (e = bh::sort_init_attributes()) != cudaSuccess ||
         (e = bh::walk_init_attributes()) != cudaSuccess ||
         (e = bh::build_init_attributes()) != cudaSuccess) {
@@ -688,6 +693,7 @@ extern "C" int bh_destroy(bh_sim* s) {
     for (int k = 0; k < kMarkers; ++k)
         if (s->markers[k]) cudaEventDestroy(s->markers[k]);
     if (s->ev_vel) cudaEventDestroy(s->ev_vel);
+    if (s->err_host) cudaFreeHost(s->err_host);
     if (s->ev_mass) cudaEventDestroy(s->ev_mass);
     if (s->ev_copy_order) cudaEventDestroy(s->ev_copy_order);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
@@ -881,8 +887,7 @@ extern "C" int bh_download(bh_sim* s, float* mass, float* pos, float* vel, uint3
         if (pos) BH_CUDA(s, cudaMemcpyAsync(pos, s->b.pos, 8 * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
         if (vel) BH_CUDA(s, cudaMemcpyAsync(vel, s->b.vel, 8 * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
     }
-    BH_CUDA(s, cudaStreamSynchronize(s->stream));
-    return check_device_errors(s);
+    return check_device_errors(s);  // one synchronisation for the copies and the error word
 }
 
 // ---- stepping --------------------------------------------------------------------
@@ -990,8 +995,7 @@ extern "C" int bh_shard_unpack(bh_sim* s, const void* chunks, uint32_t nchunks, 
 
 extern "C" int bh_sync(bh_sim* s) {
     BH_HANDLE(s);
-    BH_CUDA(s, cudaStreamSynchronize(s->stream));
-    return check_device_errors(s);
+    return check_device_errors(s);  // synchronises the stream
 }
 
 extern "C" int bh_compute_accelerations(bh_sim* s, float* acc_host) {
