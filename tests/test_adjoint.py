@@ -5,8 +5,11 @@ differences of its own loss.
 GPU: the engine's force VJP against the FP64 direct-sum VJP; the rollout
 gradient (checkpoints every 20 steps, trees rebuilt on replay) against the
 FP64 direct-sum adjoint at N = 4,096 and against central finite differences
-(h = 1e-3, FP32) of the engine's own loss.
+of the engine's own FP32 loss (4,096 bodies and the benchmark's 65,536
+bodies, both over 200 steps).
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -89,9 +92,10 @@ def test_rollout_gradient_matches_fp64_adjoint_4096(bh, orc):
     for name, g, r in (("x0", gx, rx), ("v0", gv, rv), ("m", gm, rm)):
         rel = float(np.linalg.norm(g - r) / np.linalg.norm(r))
         cos = float((g * r).sum() / (np.linalg.norm(g) * np.linalg.norm(r)))
-        print(f"rollout gradient d/d{name} vs FP64 adjoint: relative error {rel:.3e}, cosine {cos:.6f}")
-        assert rel <= 5e-2
-        assert cos > 0.995
+        print(f"rollout gradient d/d{name} vs FP64 adjoint: relative error {rel:.3e}, cosine {cos:.8f}")
+        # measured on B200: relative errors 4.4e-4 (x0), 6.5e-4 (v0), 4.8e-4 (m)
+        assert rel <= 5e-3
+        assert cos > 0.99999
     # the handle is left at step T
     _, p_end, _ = sim.download()
     assert np.isfinite(p_end).all()
@@ -99,10 +103,23 @@ def test_rollout_gradient_matches_fp64_adjoint_4096(bh, orc):
 
 
 @pytest.mark.gpu
-def test_rollout_gradient_matches_finite_differences(bh):
-    n, steps, h = 1024, 40, 1e-3
+@pytest.mark.parametrize("n,steps,leaf", [(4096, 200, 8), (65536, 200, 4)])
+def test_rollout_gradient_matches_finite_differences(bh, n, steps, leaf):
+    """Central differences of the engine's own FP32 loss along one random
+    direction per parameter block, sized per component: positions by 3e-5
+    (RMS), velocities by 3e-5 / t (a velocity change dv moves a body by dv t,
+    t = steps dt), masses by 1% of each mass.  The central difference's
+    truncation error grows as the step squared (close pairs at the softening
+    length make the loss strongly non-linear in positions: 1,024 bodies over
+    40 steps gave 3.1%, 6.0% and 83% at position steps of 2.2e-5, 3e-5 and
+    2.2e-4, while smaller steps sink into the FP32 noise of the loss over so
+    short a run), so both cases run 200 steps.  With a velocity step as small
+    as the position step the difference sat below that noise.  The
+    65,536-body case is the differentiable-rollout workload of the
+    benchmark."""
     mass, pos, vel, tgt = _target(bh, n, 9, steps)
-    sim = bh.Simulation(adjoint_config(bh))
+    cfg = dataclasses.replace(adjoint_config(bh), leafSize=leaf)
+    sim = bh.Simulation(cfg)
     sim.setNumBodies(n)
     sim.upload(mass, pos, vel)
     _, gx, gv, gm = sim.rollout_grad(steps, 20, tgt)
@@ -115,18 +132,35 @@ def test_rollout_gradient_matches_finite_differences(bh):
 
     rng = np.random.default_rng(2)
     for which in ("x", "v", "m"):
-        d = rng.normal(size=(n, 2) if which != "m" else n).astype(np.float32)
-        d /= np.linalg.norm(d)
-        if which == "m":
-            d = (d * mass / np.abs(mass).max()).astype(np.float32)
+        d = rng.normal(size=(n, 2) if which != "m" else n)
+        d /= np.sqrt((d * d).mean())  # unit RMS per component
         base = {"x": pos, "v": vel, "m": mass}[which]
-        plus, minus = base + h * d, base - h * d
+        if which == "x":
+            step = 3e-5 * d
+        elif which == "v":
+            step = 3e-5 / (steps * DT) * d
+        else:
+            step = 1e-2 * d * mass
         args = {"x": lambda a: (mass, a, vel), "v": lambda a: (mass, pos, a),
                 "m": lambda a: (a, pos, vel)}[which]
-        fd = (loss(*args(plus)) - loss(*args(minus))) / (2 * h)
-        g = {"x": gx, "v": gv, "m": gm}[which]
-        ad = float((g.astype(np.float64) * d).sum())
-        print(f"directional derivative along d{which}: adjoint {ad:.6e}, central FD {fd:.6e}, "
+        g = {"x": gx, "v": gv, "m": gm}[which].astype(np.float64)
+
+        def central(s):
+            """Half the loss difference over +-s, and the adjoint's linear
+            prediction of it for the step actually taken after FP32 rounding."""
+            plus = (base + s).astype(np.float32)
+            minus = (base - s).astype(np.float32)
+            dd = (plus.astype(np.float64) - minus.astype(np.float64)) / 2
+            return (loss(*args(plus)) - loss(*args(minus))) / 2, float((g * dd).sum())
+
+        # Richardson extrapolation over s and s/2 removes the s^3 term of the
+        # central difference: (8 F(s/2) - F(s)) / 3 is linear in s.
+        f1, a1 = central(step)
+        f2, a2 = central(step / 2)
+        fd = (8 * f2 - f1) / 3
+        ad = (8 * a2 - a1) / 3
+        print(f"n={n} T={steps}: change along d{which}: adjoint {ad:.6e}, central FD {fd:.6e} "
+              f"(extrapolated; step s alone {abs(f1 - a1) / abs(a1):.3e}), "
               f"relative difference {abs(fd - ad) / abs(ad):.3e}")
-        assert abs(fd - ad) <= 5e-2 * abs(ad) + 1e-9, (which, fd, ad)
+        assert abs(fd - ad) <= 2e-2 * abs(ad), (which, fd, ad)
     sim.close()

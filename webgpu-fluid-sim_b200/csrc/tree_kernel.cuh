@@ -121,6 +121,18 @@ constexpr int kBuildBlockSplit = BH_BUILD_BLOCK_SPLIT;
 constexpr int kClimbBlock = 256;
 template <bool SPLIT>
 constexpr int build_block() { return SPLIT ? kBuildBlockSplit : kBuildBlockFused; }
+// Resident CTAs per SM the launch bounds ask for.  The split build's local
+// phase issues in only ~60% of its cycles with 2 CTAs of 512 threads (47
+// registers); asking for 3 gives 40 registers with 16 B of spills and a
+// faster build (16.8M bodies: 1.86 -> 1.71 ms).  The fused build keeps the
+// compiler's choice (0: no minimum): 10 or 12 resident CTAs of 128 threads
+// (42-51 registers, spills) made it slower at 800k bodies (0.137 -> 0.143 /
+// 0.150 ms).
+#ifndef BH_BUILD_MIN_BLOCKS_SPLIT
+#define BH_BUILD_MIN_BLOCKS_SPLIT 3
+#endif
+template <bool SPLIT>
+constexpr int build_min_blocks() { return SPLIT ? BH_BUILD_MIN_BLOCKS_SPLIT : 0; }
 static_assert(kFp64MinBodies > kBuildBlockFused && kFp64MinBodies > kBuildBlockSplit,
               "local nodes must all take the f32 path");
 
@@ -373,10 +385,12 @@ __device__ __forceinline__ void climb(const BuildArgs<K>& A, Climb& c, BuildShar
 // which pays off from a few million bodies up (measured: 2.14 -> 1.87 ms at
 // 16.8M bodies; at 800k the extra launch costs about as much as it saves).
 // (Climbing the local phase in CTA-wide rounds that pack the remaining
-// nodes into the lowest warps measured slower: the build waits on the
-// gathers of positions and masses, not on idle lanes.)
+// nodes into the lowest warps measured slower.  Nor do the random leaf
+// gathers set the pace: with the bodies uploaded in the previous step's
+// sorted order, so the gathers run nearly in sequence, the 16.8M-body build
+// took 1.80 against 1.84 ms.)
 template <typename K, bool SPLIT>
-__global__ void __launch_bounds__(build_block<SPLIT>())
+__global__ void __launch_bounds__(build_block<SPLIT>(), build_min_blocks<SPLIT>())
 build_fill_kernel(const BuildArgs<K> A) {
     constexpr int B = build_block<SPLIT>();
     // dynamic: sizeof(BuildShared<K, B>) bytes (more than 48 KB for large B)
