@@ -81,8 +81,13 @@ struct GroupSmem {
 };
 
 // Far list: the top `cnt` (<= 32) far entries of `nf_total`, one per lane,
-// added to the lane's local-expansion sums.
-__device__ __forceinline__ void far_batch(GroupSmem<true>& S, float (&cacc)[kFarCoeffs], int lane,
+// added to the lane's local-expansion sums.  Not inlined: the coefficient
+// arithmetic is the walk's register peak, and as a call (the caller's live
+// values saved around it, the sums in a 56-B stack frame) the 128-body
+// far-field walk fits 6 blocks per SM in 80 registers instead of 5 in 96.
+// A call costs little once per 32 far nodes (800k bodies: walk 0.399 ->
+// 0.392 ms; 16.8M: 7.87 -> 7.69 ms).
+__device__ __noinline__ void far_batch(GroupSmem<true>& S, float (&cacc)[kFarCoeffs], int lane,
                                           int nf_total, int cnt, float gcx, float gcy, float lam,
                                           float eps2) {
     constexpr int cap = GroupSmem<true>::kListCap;
@@ -98,23 +103,28 @@ __device__ __forceinline__ void far_batch(GroupSmem<true>& S, float (&cacc)[kFar
 
 // Register budget: launch bounds for blocks of up to 256 threads with 3
 // resident per SM for groups of <= 64 bodies (at most 85 registers, the
-// budget of 6 resident 128-thread blocks); for 128-body groups, whose two
-// packed accumulator pairs per lane need more, blocks of up to 128 threads
-// with 5 resident (at most 102).  The bound does not depend on the block
-// shape chosen at launch (walk_block: 64, 128 or, for groups of <= 64
-// bodies, 256 threads), so the shape leaves the warps resident per SM
+// budget of 6 resident 128-thread blocks); for 128-body groups blocks of up
+// to 128 threads with 6 resident (at most 85: 80 for the far-field walk with
+// its coefficient routine called, not inlined).  The bound does not depend
+// on the block shape chosen at launch (walk_block: 64, 128 or, for groups of
+// <= 64 bodies, 256 threads), so the shape leaves the warps resident per SM
 // unchanged.  (An explicit register cap of 72 in place of these bounds gave
 // a 65-register build of the 64-body walk that ran 12% slower.)
 constexpr int walk_max_threads(int bpl) { return bpl >= 4 ? 128 : 256; }
 #ifndef BH_WALK_MIN_BLOCKS_128
-#define BH_WALK_MIN_BLOCKS_128 5
+#define BH_WALK_MIN_BLOCKS_128 6
 #endif
 constexpr int walk_min_blocks(int bpl) { return bpl >= 4 ? BH_WALK_MIN_BLOCKS_128 : 3; }
 
 // FAR: the far-field variant (Plummer softening, quadrupoles); the other
-// instantiations carry none of its code or registers.  Shared memory: one
-// GroupSmem<FAR> per warp, dynamic (the block shape is chosen at launch).
-template <int BPL, int MP, bool PLUMMER, bool FAR>
+// instantiations carry none of its code or registers.  COUNT: the
+// instrumented walk of bh_walk_stats, which also counts node visits and
+// interactions; the stepping walk carries no counters (as a runtime switch
+// their four 64-bit sums held 8 registers through the whole traversal and
+// cost 5% at 800k and 16.8M bodies, 8% for 64-body groups).  Shared memory:
+// one GroupSmem<FAR> per warp, dynamic (the block shape is chosen at
+// launch).
+template <int BPL, int MP, bool PLUMMER, bool FAR, bool COUNT>
 __global__ void __launch_bounds__(walk_max_threads(BPL), walk_min_blocks(BPL))
 walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ node4,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ ids,
@@ -134,7 +144,7 @@ walk_group_kernel(const GNode* __restrict__ gnode, const float4* __restrict__ no
     const float eps2 = P.eps2, ecoef = P.eps_coef;
     // With a positive softening the own-leaf term is exactly zero.
     const bool self_test = !(PLUMMER && eps2 > 0.0f);
-    const bool counting = P.count != 0;
+    constexpr bool counting = COUNT;
     unsigned long long c_vis = 0, c_node = 0, c_body = 0, c_far = 0;
     const int stack_cap = (P.stack_cap > 0 && P.stack_cap < kWalkStack) ? P.stack_cap : kWalkStack;
 
@@ -535,24 +545,27 @@ static int shape_index(int warps) { return warps == 2 ? 0 : (warps == 8 ? 2 : 1)
 
 template <int BPL, int MP, bool PL, bool FAR>
 static cudaError_t set_walk_attributes() {
-    return cudaFuncSetAttribute(walk_group_kernel<BPL, MP, PL, FAR>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(walk_max_threads(BPL) / 32 * sizeof(GroupSmem<FAR>)));
+    const int smem = (int)(walk_max_threads(BPL) / 32 * sizeof(GroupSmem<FAR>));
+    cudaError_t e = cudaFuncSetAttribute(walk_group_kernel<BPL, MP, PL, FAR, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(walk_group_kernel<BPL, MP, PL, FAR, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
 // Largest walk block for bodies_per_lane `bpl` (its launch bound).
 int walk_group_max_block(int bpl) { return walk_max_threads(bpl >= 4 ? 4 : 2); }
 
-template <int BPL, int MP, bool PL, bool FAR = false>
-static void launch_t(const DeviceBuffers& b, const WalkParams& p, int warps, cudaStream_t s) {
+template <int BPL, int MP, bool PL, bool FAR, bool COUNT>
+static void launch_c(const DeviceBuffers& b, const WalkParams& p, int warps, cudaStream_t s) {
     static int blocks_per_sm[64][3] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     const size_t smem = (size_t)warps * sizeof(GroupSmem<FAR>);
     int& bps = blocks_per_sm[dev & 63][shape_index(warps)];
     if (bps == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, walk_group_kernel<BPL, MP, PL, FAR>,
-                                                      warps * 32, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &bps, walk_group_kernel<BPL, MP, PL, FAR, COUNT>, warps * 32, smem);
         if (bps < 1) bps = 1;
     }
     int sms = 148;
@@ -562,8 +575,15 @@ static void launch_t(const DeviceBuffers& b, const WalkParams& p, int warps, cud
     const uint32_t need = (b.n + warps - 1) / warps;
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
-    walk_group_kernel<BPL, MP, PL, FAR><<<blocks, warps * 32, smem, s>>>(
+    walk_group_kernel<BPL, MP, PL, FAR, COUNT><<<blocks, warps * 32, smem, s>>>(
         b.gnode, b.node4, b.groups, b.ids, b.pos, b.vel, b.acc, p, b.err);
+}
+
+// The counting walk only when bh_walk_stats asks for it (p.count).
+template <int BPL, int MP, bool PL, bool FAR = false>
+static void launch_t(const DeviceBuffers& b, const WalkParams& p, int warps, cudaStream_t s) {
+    if (p.count) launch_c<BPL, MP, PL, FAR, true>(b, p, warps, s);
+    else launch_c<BPL, MP, PL, FAR, false>(b, p, warps, s);
 }
 
 template <int BPL>
