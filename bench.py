@@ -55,7 +55,7 @@ DEFAULT_WORKLOAD = "colliding-disks-800k"
 FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes (read + write) of one launch of the dominant kernel (the walk),
 # from one ncu capture of the same workload.
-NCU_WALK_TRAFFIC_BYTES = {"colliding-disks-800k": 44.16e6}
+NCU_WALK_TRAFFIC_BYTES = {"colliding-disks-800k": 72.04e6}  # far-field walk, 128-body groups
 # Algorithmic HBM bytes per body and step of the stream stages: encode =
 # position 8 + mass 4 read, key 4|8 + packed leaf record 16 written; sort =
 # first pass key read + key and id written, later passes key and id read and
