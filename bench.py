@@ -12,7 +12,9 @@ Own arm (default):
              between timed steps (flush outside the timed events).
   e2e        the same metric through the public API with host buffers: per
              step upload(mass, pos, vel) from page-locked memory, one step,
-             download(pos, vel) into page-locked memory.
+             download(pos, vel) into page-locked memory -- pipelined (the
+             download asynchronous, one sync after the loop); the same loop
+             with every download waiting is reported beside it ("serial").
   roofline   the dominant kernel (walk), from per-stage CUDA events recorded
              in the step graph during the timed steps.
   cpu_baseline  the oracle (C restatement, OpenMP, all host threads) on a
@@ -198,10 +200,14 @@ def stream_rooflines(stages: dict, n: int, key_bytes: int, hbm_gbs: float) -> di
 
 
 def e2e_rate(sim, step, n: int, steps: int, ext, barrier=lambda: None, dist=None, units=None):
-    """The metric through the public API with host buffers: per step, upload
-    masses, positions and velocities from page-locked memory, one step,
-    download positions and velocities into page-locked memory; CUDA events on
-    the engine's stream around the whole loop."""
+    """The metric through the public API with host buffers: every step
+    uploads masses, positions and velocities from page-locked memory, runs
+    one step and downloads positions and velocities into page-locked memory.
+    Two loops over the same calls, CUDA events on the engine's stream around
+    each: pipelined (the download is asynchronous and nothing waits inside
+    the loop, so step k's download and step k+1's position upload overlap
+    the neighbouring steps; one sync after the loop, inside the events) and
+    serial (every download waits before the next upload is issued)."""
     import torch
     mass, pos, vel = sim.download()
     h_mass = torch.from_numpy(mass).pin_memory()
@@ -212,23 +218,36 @@ def e2e_rate(sim, step, n: int, steps: int, ext, barrier=lambda: None, dist=None
     sim.upload(h_mass, h_pos, h_vel)
     step(1)
     sim.download_into(None, o_pos, o_vel)
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(ext)
-    for _ in range(steps):
-        sim.upload(h_mass, h_pos, h_vel)
-        step(1)
-        sim.download_into(None, o_pos, o_vel)  # synchronises the stream
-    e1.record(ext)
-    e1.synchronize()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device=torch.device("cuda", sim.device))
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return {"value": (units or n) * steps / (float(t.item()) / 1e3), "unit": "body-steps/s",
+
+    def timed(wait: bool) -> float:
+        sim.sync()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        for _ in range(steps):
+            sim.upload(h_mass, h_pos, h_vel)
+            step(1)
+            sim.download_into(None, o_pos, o_vel, wait=wait)
+        sim.sync()  # the last download has reached the host
+        e1.record(ext)
+        e1.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64,
+                         device=torch.device("cuda", sim.device))
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms_pipe = timed(wait=False)
+    ms_serial = timed(wait=True)
+    rate = lambda ms: (units or n) * steps / (ms / 1e3)
+    return {"value": rate(ms_pipe), "unit": "body-steps/s",
             "h2d_bytes_per_step": int(h_mass.nbytes + h_pos.nbytes + h_vel.nbytes),
-            "d2h_bytes_per_step": int(o_pos.nbytes + o_vel.nbytes), "steps": steps}
+            "d2h_bytes_per_step": int(o_pos.nbytes + o_vel.nbytes), "steps": steps,
+            "ms_per_step": ms_pipe / steps,
+            "loop": "pipelined: upload, step, asynchronous download per step; one sync after the loop",
+            "serial": {"value": rate(ms_serial), "ms_per_step": ms_serial / steps,
+                       "loop": "every download waits before the next upload"}}
 
 
 def secondary_16m(pkg, device: int, steps: int = 5, e2e_steps: int = 3, sm_max_mhz=None,

@@ -115,14 +115,26 @@ int bh_update_metadata(bh_sim* sim);
  * checkpoint path).  n must equal the body count.  Any pointer may be NULL
  * to skip that array.  bh_upload is asynchronous for page-locked host
  * memory, which must stay valid until the copies are done (the next
- * bh_sync or bh_download): positions are copied on the handle's stream,
- * masses and then velocities on a second copy stream of the handle, ordered
- * after everything enqueued before.  The next step's stages before their
- * first reader (the hierarchy build for the masses, the walk for the
- * velocities) do not wait for them; every other call orders the handle's
- * stream after them.  bh_download synchronises before returning. */
+ * bh_sync or bh_download).  The copies run on a second copy stream of the
+ * handle: positions into a device staging buffer at once (they may overlap
+ * steps still running; the handle's stream moves them into place before
+ * their next reader), then masses and velocities, ordered after everything
+ * enqueued before.  The next step's stages before their first reader (the
+ * hierarchy build for the masses, the walk for the velocities) do not wait
+ * for them; every other call orders the handle's stream after them.
+ * bh_download synchronises before returning. */
 int bh_upload(bh_sim* sim, const float* mass, const float* pos, const float* vel, uint32_t n);
 int bh_download(bh_sim* sim, float* mass, float* pos, float* vel, uint32_t n);
+
+/* Same as bh_download, without waiting (extension; no reference counterpart
+ * beyond the readback of simulation.ts:376-384).  The arrays are copied on
+ * the handle's stream into a device snapshot, and from there to the host on
+ * a third stream of the handle, so the steps enqueued next run while the
+ * host copy is under way.  The host arrays (page-locked for an asynchronous
+ * copy) are written by the next bh_sync or bh_download, which wait for the
+ * copy and report device errors; a later bh_download_async reuses the
+ * snapshot once this copy has left it. */
+int bh_download_async(bh_sim* sim, float* mass, float* pos, float* vel, uint32_t n);
 
 /* getCommands() + queue.submit (simulation.ts:386-425, main.ts:38-41):
  * enqueue `frames` frames of config.substeps steps each.  Asynchronous. */

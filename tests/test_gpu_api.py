@@ -181,8 +181,8 @@ def test_velocity_upload_overlap_on_an_ensemble(bh):
 
 @pytest.mark.parametrize("n", [1, 2, 300, 12000])
 def test_partial_uploads_overlapping_the_step(bh, n):
-    """Uploads of some arrays only (masses and velocities travel on the copy
-    stream, positions on the handle's stream), each followed by a step:
+    """Uploads of some arrays only (all travel on the copy stream, the
+    positions through the staging buffer), each followed by a step:
     bit-equal to waiting for the upload, down to one and two bodies."""
     cfg = dict(walk="group", softening="plummer", plummerEps=1e-3, mortonDomain="bbox",
                integrator="symplectic-euler", deltaTime=1e-3)
@@ -204,3 +204,87 @@ def test_partial_uploads_overlapping_the_step(bh, n):
         assert np.array_equal(x, y)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("integrator,walk,n", [("symplectic-euler", "group", 20000),
+                                               ("symplectic-euler", "exact", 20000),
+                                               ("leapfrog-kdk", "group", 20000),
+                                               ("symplectic-euler", "group", 1),
+                                               ("symplectic-euler", "group", 300)])
+def test_pipelined_round_trips_equal_serial(bh, integrator, walk, n):
+    """Upload, step and asynchronous download per step with no wait in the
+    loop: the staged positions of step k+1 cross PCIe while step k runs and
+    the download of step k while step k+1 runs.  Every step's downloaded
+    state equals a handle that waits for each copy."""
+    cfg = dict(integrator=integrator, walk=walk, softening="plummer", plummerEps=1e-3,
+               mortonDomain="bbox", deltaTime=1e-3)
+    a = _sim(bh, n=n, **cfg)
+    b = _sim(bh, n=n, **cfg)
+    m, p, v = a.download()
+    inputs = [(_pinned(m * (1.0 + 0.1 * k)), _pinned(p * (1.0 + 0.01 * k)), _pinned(v * (1.0 - 0.2 * k)))
+              for k in range(4)]
+    outs = [(_pinned(np.zeros_like(p)), _pinned(np.zeros_like(v))) for _ in inputs]
+    for (hm, hp, hv), (op, ov) in zip(inputs, outs):
+        a.upload(hm, hp, hv)
+        a.step(1)
+        a.download_into(None, op, ov, wait=False)
+    a.sync()
+    for (hm, hp, hv), (op, ov) in zip(inputs, outs):
+        b.upload(hm, hp, hv)
+        b.sync()
+        b.step(1)
+        _, pb, vb = b.download()
+        assert np.array_equal(op.numpy(), pb)
+        assert np.array_equal(ov.numpy(), vb)
+    a.close()
+    b.close()
+
+
+def test_stepping_with_asynchronous_downloads_into_one_buffer(bh):
+    """A trajectory recorded through one pair of host arrays: the downloads
+    are written in call order, so after the sync they hold the last step;
+    a waiting download after an asynchronous one sees the same state."""
+    cfg = dict(walk="group", softening="plummer", plummerEps=1e-3, mortonDomain="bbox",
+               integrator="symplectic-euler", deltaTime=1e-3)
+    a = _sim(bh, n=5000, **cfg)
+    b = _sim(bh, n=5000, **cfg)
+    _, p, v = a.download()
+    op, ov, om = _pinned(np.zeros_like(p)), _pinned(np.zeros_like(v)), _pinned(np.zeros(5000))
+    for _ in range(5):
+        a.step(1)
+        a.download_into(om, op, ov, wait=False)
+    a.sync()
+    b.step(5)
+    mb, pb, vb = b.download()
+    assert np.array_equal(op.numpy(), pb) and np.array_equal(ov.numpy(), vb)
+    assert np.array_equal(om.numpy(), mb)
+    a.step(1)
+    a.download_into(None, op, None, wait=False)
+    _, pa, _ = a.download()    # waits for the asynchronous copy first
+    b.step(1)
+    assert np.array_equal(pa, b.download()[1])
+    assert np.array_equal(op.numpy(), pa)
+    a.close()
+    b.close()
+
+
+def test_asynchronous_download_then_other_calls(bh):
+    """A body-count change, a borrowed-buffer read and closing the handle
+    while an asynchronous download may still be copying."""
+    s = _sim(bh, n=4000)
+    _, p, _ = s.download()
+    op = _pinned(np.zeros_like(p))
+    s.download_into(None, op, None, wait=False)
+    assert np.array_equal(s.read_buffer("pos", np.float32, 8000).reshape(-1, 2), p)
+    s.sync()
+    assert np.array_equal(op.numpy(), p)
+    s.download_into(None, op, None, wait=False)
+    s.setNumBodies(3000)       # reallocates while the copy may be in flight
+    s.step(1)
+    assert s.download()[1].shape == (3000, 2)
+    q = _pinned(np.zeros((3000, 2)))
+    s.step(1)
+    s.download_into(None, q, None, wait=False)
+    s.close()                  # waits for the copy before freeing anything
+    with pytest.raises(Exception):
+        s.download_into(None, q, None, wait=False)  # closed handle

@@ -114,6 +114,7 @@ SIGNATURES = {
     "bh_update_metadata": (ctypes.c_int, [_P]),
     "bh_upload": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_uint32]),
     "bh_download": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_uint32]),
+    "bh_download_async": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_uint32]),
     "bh_step": (ctypes.c_int, [_P, ctypes.c_uint32]),
     "bh_sync": (ctypes.c_int, [_P]),
     "bh_compute_accelerations": (ctypes.c_int, [_P, _P]),

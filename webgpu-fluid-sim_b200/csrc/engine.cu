@@ -48,12 +48,29 @@ struct bh_sim {
     static constexpr int kGraphs = 6;
     cudaGraph_t graph[kGraphs] = {};
     cudaGraphExec_t exec[kGraphs] = {};
-    // Uploaded masses and velocities cross PCIe on copy_stream, ordered after
-    // the stream's earlier work (ev_copy_order); the stream waits on ev_mass /
-    // ev_vel before the next use of those arrays (settle_uploads).
+    // Uploads are staged: bh_upload copies each array into its staging
+    // buffer on copy_stream as soon as the last staged copy of that array has
+    // been moved out (Staged::freed), so the copy may overlap steps still
+    // running; the handle's stream waits on Staged::landed and moves the
+    // array into place before its next reader (settle_*).
     cudaStream_t copy_stream = nullptr;
-    cudaEvent_t ev_copy_order = nullptr, ev_mass = nullptr, ev_vel = nullptr;
-    mutable bool mass_pending = false, vel_pending = false;
+    struct Staged {
+        void* buf = nullptr;  // staging buffer (in the arena)
+        size_t width = 0;     // bytes per body
+        cudaEvent_t landed = nullptr, freed = nullptr;
+        mutable bool pending = false;
+    };
+    enum { kPos = 0, kMass = 1, kVel = 2 };
+    Staged up[3];
+    // bh_download_async: the requested arrays are copied on the handle's
+    // stream into a device snapshot (ev_snap_ready), and from there to the
+    // host on d2h_stream (ev_snap_free), so the next steps need not wait for
+    // the host copy.
+    float* snap_mass = nullptr;
+    float2 *snap_pos = nullptr, *snap_vel = nullptr;
+    cudaStream_t d2h_stream = nullptr;
+    cudaEvent_t ev_snap_ready = nullptr, ev_snap_free = nullptr;
+    mutable bool snap_busy = false;
     cudaGraphNode_t ev_node[kMarkers] = {};
     cudaEvent_t markers[kMarkers] = {};
     // profiling
@@ -85,21 +102,23 @@ struct bh_sim {
 
 static thread_local std::string g_err;
 
-// Order the handle's stream after mass / velocity uploads still in flight on
-// the copy stream.  Every entry point calls settle_uploads (through
-// BH_HANDLE) before it touches the body buffers, except bh_upload and
-// bh_step, which order the copies themselves.
-static void settle_mass(const bh_sim* s) {
-    if (!s->mass_pending) return;
-    cudaStreamWaitEvent(s->stream, s->ev_mass, 0);
-    s->mass_pending = false;
+// Order the handle's stream after uploads still in flight on the copy
+// stream.  Every entry point calls settle_uploads (through BH_HANDLE) before
+// it touches the body buffers, except bh_upload and bh_step, which order the
+// copies themselves.
+static void settle(const bh_sim* s, int k, void* dst) {
+    const bh_sim::Staged& u = s->up[k];
+    if (!u.pending) return;
+    cudaStreamWaitEvent(s->stream, u.landed, 0);
+    cudaMemcpyAsync(dst, u.buf, u.width * (size_t)s->b.n, cudaMemcpyDeviceToDevice, s->stream);
+    cudaEventRecord(u.freed, s->stream);
+    u.pending = false;
 }
-static void settle_vel(const bh_sim* s) {
-    if (!s->vel_pending) return;
-    cudaStreamWaitEvent(s->stream, s->ev_vel, 0);
-    s->vel_pending = false;
-}
+static void settle_pos(const bh_sim* s) { settle(s, bh_sim::kPos, s->b.pos); }
+static void settle_mass(const bh_sim* s) { settle(s, bh_sim::kMass, s->b.mass); }
+static void settle_vel(const bh_sim* s) { settle(s, bh_sim::kVel, s->b.vel); }
 static void settle_uploads(const bh_sim* s) {
+    settle_pos(s);
     settle_mass(s);
     settle_vel(s);
 }
@@ -114,6 +133,7 @@ namespace bh {
 // refreshes the reference node layout); false for a null handle.
 bool sim_body_view(const bh_sim* s, BodyView* out) {
     if (!s || !out) return false;
+    cudaSetDevice(s->device);  // settling may copy staged positions on the handle's stream
     settle_uploads(s);  // callers use the buffers on the handle's stream
     out->mass = s->b.mass;
     out->pos = s->b.pos;
@@ -271,8 +291,16 @@ static int save_tree(bh_sim* s, uint32_t k) {
 }
 
 static void free_buffers(bh_sim* s) {
-    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);  // no copy into freed memory
-    s->mass_pending = s->vel_pending = false;
+    // no copy into or out of freed memory
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
+    if (s->d2h_stream) cudaStreamSynchronize(s->d2h_stream);
+    s->snap_busy = false;
+    for (auto& u : s->up) {
+        u.pending = false;
+        u.buf = nullptr;
+    }
+    s->snap_pos = s->snap_vel = nullptr;
+    s->snap_mass = nullptr;
     destroy_graphs(s);
     free_adjoint(s);
     if (s->arena) cudaFree(s->arena);
@@ -315,6 +343,10 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     size_t o_err = c.take<uint32_t>(1);
     size_t o_soff = E ? c.take<uint32_t>(E + 1) : 0, o_bsys = E ? c.take<uint32_t>(nb) : 0;
     size_t o_sbox = E ? c.take<uint32_t>(4 * (size_t)E) : 0;
+    // staged uploads and the asynchronous download's snapshot
+    size_t o_stpos = c.take<float2>(nb), o_stmass = c.take<float>(nb), o_stvel = c.take<float2>(nb);
+    size_t o_smass = c.take<float>(nb);
+    size_t o_spos = c.take<float2>(nb), o_svel = c.take<float2>(nb);
     void* arena = nullptr;
     cudaError_t e = cudaMalloc(&arena, c.off);
     if (e != cudaSuccess) {
@@ -355,6 +387,15 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     b.err = (uint32_t*)(a + o_err);
     b.spin_cap = s->debug_spin_cap ? s->debug_spin_cap : bh::kSpinCapDefault;
     b.debug_flags = s->debug_flags;
+    s->up[bh_sim::kPos].buf = a + o_stpos;
+    s->up[bh_sim::kPos].width = sizeof(float2);
+    s->up[bh_sim::kMass].buf = a + o_stmass;
+    s->up[bh_sim::kMass].width = sizeof(float);
+    s->up[bh_sim::kVel].buf = a + o_stvel;
+    s->up[bh_sim::kVel].width = sizeof(float2);
+    s->snap_mass = (float*)(a + o_smass);
+    s->snap_pos = (float2*)(a + o_spos);
+    s->snap_vel = (float2*)(a + o_svel);
     BH_CUDA(s, cudaMemsetAsync(arena, 0, c.off, s->stream));
     BH_CUDA(s, cudaMemsetAsync(b.bound, 0xFF, sizeof(uint32_t) * ni, s->stream));
     if (E) {
@@ -546,9 +587,12 @@ static cudaEvent_t* prof_slot(bh_sim* s) {
 // Synchronises the handle's stream once, after the work the caller enqueued
 // and a copy of the device error word into page-locked host memory.
 static int check_device_errors(bh_sim* s) {
+    // an asynchronous download still copying to the host finishes first
+    if (s->snap_busy) BH_CUDA(s, cudaStreamWaitEvent(s->stream, s->ev_snap_free, 0));
     BH_CUDA(s, cudaMemcpyAsync(s->err_host, s->b.err, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                s->stream));
     BH_CUDA(s, cudaStreamSynchronize(s->stream));
+    s->snap_busy = false;
     const uint32_t e = *s->err_host;
     if (e == 0) return BH_OK;
     BH_CUDA(s, cudaMemsetAsync(s->b.err, 0, sizeof(uint32_t), s->stream));
@@ -648,9 +692,15 @@ static int create_sim(const bh_config* config, const uint32_t* sizes, uint32_t n
     if ((e = cudaSetDevice(s->device)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&s->ev_copy_order, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&s->ev_mass, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&s->ev_vel, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&s->up[0].landed, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&s->up[0].freed, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&s->up[1].landed, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&s->up[1].freed, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&s->up[2].landed, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&s->up[2].freed, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&s->d2h_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&s->ev_snap_ready, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&s->ev_snap_free, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaHostAlloc((void**)&s->err_host, sizeof(uint32_t), cudaHostAllocDefault)) != cudaSuccess ||
         (e = bh::sort_init_attributes()) != cudaSuccess ||
         (e = bh::walk_init_attributes()) != cudaSuccess ||
@@ -692,10 +742,14 @@ extern "C" int bh_destroy(bh_sim* s) {
     free_profile(s);
     for (int k = 0; k < kMarkers; ++k)
         if (s->markers[k]) cudaEventDestroy(s->markers[k]);
-    if (s->ev_vel) cudaEventDestroy(s->ev_vel);
     if (s->err_host) cudaFreeHost(s->err_host);
-    if (s->ev_mass) cudaEventDestroy(s->ev_mass);
-    if (s->ev_copy_order) cudaEventDestroy(s->ev_copy_order);
+    for (auto& u : s->up) {
+        if (u.landed) cudaEventDestroy(u.landed);
+        if (u.freed) cudaEventDestroy(u.freed);
+    }
+    if (s->ev_snap_ready) cudaEventDestroy(s->ev_snap_ready);
+    if (s->ev_snap_free) cudaEventDestroy(s->ev_snap_free);
+    if (s->d2h_stream) cudaStreamDestroy(s->d2h_stream);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -855,25 +909,18 @@ extern "C" int bh_upload(bh_sim* s, const float* mass, const float* pos, const f
     BH_HANDLE_NO_SETTLE(s);
     if (n != s->b.n) return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_upload: n differs from the body count");
     if (n == 0) return BH_OK;
-    if (pos) BH_CUDA(s, cudaMemcpyAsync(s->b.pos, pos, 8 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
-    if (mass || vel) {
-        // On the copy stream, after everything enqueued so far on the handle's
-        // stream (so after the position copy, and after any step still
-        // reading the masses or reading or writing the velocities): masses,
-        // then velocities.  The next step's stages before their first reader
-        // do not wait for them (step_once); every other call does.
-        BH_CUDA(s, cudaEventRecord(s->ev_copy_order, s->stream));
-        BH_CUDA(s, cudaStreamWaitEvent(s->copy_stream, s->ev_copy_order, 0));
-        if (mass) {
-            BH_CUDA(s, cudaMemcpyAsync(s->b.mass, mass, 4 * (size_t)n, cudaMemcpyHostToDevice, s->copy_stream));
-            BH_CUDA(s, cudaEventRecord(s->ev_mass, s->copy_stream));
-            s->mass_pending = true;
-        }
-        if (vel) {
-            BH_CUDA(s, cudaMemcpyAsync(s->b.vel, vel, 8 * (size_t)n, cudaMemcpyHostToDevice, s->copy_stream));
-            BH_CUDA(s, cudaEventRecord(s->ev_vel, s->copy_stream));
-            s->vel_pending = true;
-        }
+    // Each array into its staging buffer on the copy stream, once the last
+    // staged copy of that array has been moved out: the copies need not wait
+    // for steps still running.  Positions first (the step's first reader),
+    // then masses (the build), then velocities (the walk).
+    const void* src[3] = {pos, mass, vel};
+    for (int k : {(int)bh_sim::kPos, (int)bh_sim::kMass, (int)bh_sim::kVel}) {
+        bh_sim::Staged& u = s->up[k];
+        if (!src[k]) continue;
+        BH_CUDA(s, cudaStreamWaitEvent(s->copy_stream, u.freed, 0));
+        BH_CUDA(s, cudaMemcpyAsync(u.buf, src[k], u.width * (size_t)n, cudaMemcpyHostToDevice, s->copy_stream));
+        BH_CUDA(s, cudaEventRecord(u.landed, s->copy_stream));
+        u.pending = true;
     }
     if (mass || pos) s->acc_valid = false;
     return BH_OK;
@@ -883,6 +930,8 @@ extern "C" int bh_download(bh_sim* s, float* mass, float* pos, float* vel, uint3
     BH_HANDLE(s);
     if (n != s->b.n) return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_download: n differs from the body count");
     if (n) {
+        // host arrays are written in call order: after an earlier asynchronous download
+        if (s->snap_busy) BH_CUDA(s, cudaStreamWaitEvent(s->stream, s->ev_snap_free, 0));
         if (mass) BH_CUDA(s, cudaMemcpyAsync(mass, s->b.mass, 4 * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
         if (pos) BH_CUDA(s, cudaMemcpyAsync(pos, s->b.pos, 8 * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
         if (vel) BH_CUDA(s, cudaMemcpyAsync(vel, s->b.vel, 8 * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
@@ -890,26 +939,49 @@ extern "C" int bh_download(bh_sim* s, float* mass, float* pos, float* vel, uint3
     return check_device_errors(s);  // one synchronisation for the copies and the error word
 }
 
+extern "C" int bh_download_async(bh_sim* s, float* mass, float* pos, float* vel, uint32_t n) {
+    BH_HANDLE(s);
+    if (n != s->b.n)
+        return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_download_async: n differs from the body count");
+    if (n == 0 || !(mass || pos || vel)) return BH_OK;
+    // The snapshot is reused once the previous asynchronous download has
+    // copied it to the host.
+    if (s->snap_busy) BH_CUDA(s, cudaStreamWaitEvent(s->stream, s->ev_snap_free, 0));
+    if (mass) BH_CUDA(s, cudaMemcpyAsync(s->snap_mass, s->b.mass, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s->stream));
+    if (pos) BH_CUDA(s, cudaMemcpyAsync(s->snap_pos, s->b.pos, 8 * (size_t)n, cudaMemcpyDeviceToDevice, s->stream));
+    if (vel) BH_CUDA(s, cudaMemcpyAsync(s->snap_vel, s->b.vel, 8 * (size_t)n, cudaMemcpyDeviceToDevice, s->stream));
+    BH_CUDA(s, cudaEventRecord(s->ev_snap_ready, s->stream));
+    BH_CUDA(s, cudaStreamWaitEvent(s->d2h_stream, s->ev_snap_ready, 0));
+    if (mass) BH_CUDA(s, cudaMemcpyAsync(mass, s->snap_mass, 4 * (size_t)n, cudaMemcpyDeviceToHost, s->d2h_stream));
+    if (pos) BH_CUDA(s, cudaMemcpyAsync(pos, s->snap_pos, 8 * (size_t)n, cudaMemcpyDeviceToHost, s->d2h_stream));
+    if (vel) BH_CUDA(s, cudaMemcpyAsync(vel, s->snap_vel, 8 * (size_t)n, cudaMemcpyDeviceToHost, s->d2h_stream));
+    BH_CUDA(s, cudaEventRecord(s->ev_snap_free, s->d2h_stream));
+    s->snap_busy = true;
+    return BH_OK;
+}
+
 // ---- stepping --------------------------------------------------------------------
 
 static int step_once(bh_sim* s) {
     const bool kdk = s->cfg.integrator == BH_INTEGRATOR_LEAPFROG_KDK;
     cudaEvent_t* ev = prof_slot(s);
-    const bool overlap = (s->mass_pending || s->vel_pending) && !kdk && !ev && s->cfg.use_graphs;
+    settle_pos(s);  // the reset and bounding box come first: positions are read at once
+    const bool overlap = (s->up[bh_sim::kMass].pending || s->up[bh_sim::kVel].pending) && !kdk && !ev &&
+                         s->cfg.use_graphs;
     if (!overlap) settle_uploads(s);  // leapfrog reads both at once (force evaluation, opening kick)
     if (kdk && !s->acc_valid) {
         enqueue_forces(s, [](int) {});  // first force evaluation of a leapfrog run
         s->acc_valid = true;
     }
     if (overlap) {
-        // The last upload's masses and velocities are still crossing PCIe on
-        // the copy stream (masses first).  The build is the masses' first
+        // The last upload's masses and velocities may still be crossing PCIe
+        // into their staging buffers (masses first).  The build is the masses' first
         // reader and the walk the velocities', so the stages before them run
         // meanwhile: the same kernels in the same order as the whole-step
         // graph, except that with masses pending the encode writes no packed
         // leaf records and the build gathers masses and positions instead
         // (the same values).
-        const bool m = s->mass_pending;
+        const bool m = s->up[bh_sim::kMass].pending;
         const int need[3] = {m ? 4 : 2, m ? 5 : 3, 3};
         for (int v : need)
             if (!s->exec[v]) {

@@ -180,11 +180,20 @@ class Simulation:
         self._pending_host = []
         return mass, pos, vel
 
-    def download_into(self, mass=None, pos=None, vel=None) -> None:
-        """Download into caller-owned host arrays (page-locked for async speed)."""
+    def download_into(self, mass=None, pos=None, vel=None, wait: bool = True) -> None:
+        """Download into caller-owned host arrays (page-locked for async speed).
+
+        wait=False returns at once (bh_download_async): the arrays are written
+        by the next sync() or waiting download, and the steps enqueued
+        meanwhile run while the copy is under way."""
         n = self.getNumBodies()
-        self._check(self._lib.bh_download(self._h, _ptr(mass), _ptr(pos), _ptr(vel), n))
-        self._pending_host = []
+        if wait:
+            self._check(self._lib.bh_download(self._h, _ptr(mass), _ptr(pos), _ptr(vel), n))
+            self._pending_host = []
+            return
+        self._check(self._lib.bh_download_async(self._h, _ptr(mass), _ptr(pos), _ptr(vel), n))
+        # the host arrays must outlive the copy: held until the next sync
+        self._pending_host = getattr(self, "_pending_host", []) + [[mass, pos, vel]]
 
     def computeAccelerations(self) -> np.ndarray:
         n = self.getNumBodies()
