@@ -116,12 +116,12 @@ int bh_update_metadata(bh_sim* sim);
  * to skip that array.  bh_upload is asynchronous for page-locked host
  * memory, which must stay valid until the copies are done (the next
  * bh_sync or bh_download).  The copies run on a second copy stream of the
- * handle, positions, masses, velocities, each into a device staging buffer
- * as soon as the previous staged copy of that array has been moved into
- * place, so they may overlap steps still running.  The handle's stream
- * moves each array into place before its next reader: the next step's
- * stages before that reader (the hierarchy build for the masses, the walk
- * for the velocities) do not wait for it; every other call waits first.
+ * handle: positions into a device staging buffer at once (they may overlap
+ * steps still running; the handle's stream moves them into place before
+ * their next reader), then masses and velocities, ordered after everything
+ * enqueued before.  The next step's stages before their first reader (the
+ * hierarchy build for the masses, the walk for the velocities) do not wait
+ * for them; every other call orders the handle's stream after them.
  * bh_download synchronises before returning. */
 int bh_upload(bh_sim* sim, const float* mass, const float* pos, const float* vel, uint32_t n);
 int bh_download(bh_sim* sim, float* mass, float* pos, float* vel, uint32_t n);
@@ -457,16 +457,9 @@ const char* bh_renderer_last_error(bh_renderer* r);
  *   walk_stack_cap     stack entries a walk warp may use (0 = full; >= 2)
  *   flags              BH_DEBUG_LOOKBACK_UNPUBLISHED: the second tile of the
  *                      first sort pass waits on a predecessor status that
- *                      never reads as published (needs n > 6144 bodies);
- *                      BH_DEBUG_UPPER_CAP_SMALL: the hierarchy build's upper
- *                      levels combine at most 64 nodes per CTA and hand
- *                      larger runs to the device-scope climb;
- *                      BH_DEBUG_SPLIT_BUILD: the split hierarchy build (local
- *                      phase, upper levels, climb) at every body count
+ *                      never reads as published (needs n > 6144 bodies)
  * Zeros restore normal operation.  Takes effect from the next call. */
 #define BH_DEBUG_LOOKBACK_UNPUBLISHED 1u
-#define BH_DEBUG_UPPER_CAP_SMALL 2u
-#define BH_DEBUG_SPLIT_BUILD 4u
 int bh_debug_set_limits(bh_sim* sim, uint32_t flags, uint32_t lookback_spin_cap,
                         uint32_t walk_stack_cap);
 

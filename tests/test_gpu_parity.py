@@ -52,15 +52,6 @@ def compare_tree(orc, sim, check_values=True):
     return acc, acc_ref
 
 
-def split_build_kernels(n, local_block=512, runs_per_cta=128):
-    """Kernels of the split hierarchy build: the local phase, one upper level
-    per factor of runs_per_cta CTAs, the device-scope climb."""
-    ctas, levels = -(-n // local_block), 0
-    while ctas > 1:
-        ctas, levels = -(-ctas // runs_per_cta), levels + 1
-    return 2 + levels
-
-
 def acc_errors(acc, acc_ref):
     num = np.linalg.norm(acc.astype(np.float64) - acc_ref, axis=1)
     den = np.linalg.norm(acc_ref.astype(np.float64), axis=1)
@@ -163,11 +154,9 @@ def test_split_build_matches_oracle_beyond_2m(bh, orc, cfg):
     # the frontier nodes it leaves; both node layouts against the oracle.
     n = (1 << 21) + 4097
     sim = make_sim(bh, n, "gaussian-mixture", seed=3, **cfg)
-    # reset, bbox, encode, sort passes, build (local phase, upper levels,
-    # device-scope climb), walk
-    assert sim.kernels_per_step() == (1 + 1 + 1 + 8 + split_build_kernels(n) + 1
-                                      if cfg.get("mortonBits") == 64
-                                      else 1 + 1 + 1 + 4 + split_build_kernels(n) + 1)
+    # reset, bbox, encode, sort passes, build (2 kernels), walk
+    assert sim.kernels_per_step() == (1 + 1 + 1 + 8 + 2 + 1 if cfg.get("mortonBits") == 64
+                                      else 1 + 1 + 1 + 4 + 2 + 1)
     mass, pos, vel = sim.download()
     sim.computeAccelerations()
     t = sim.tree()
@@ -188,61 +177,6 @@ def test_split_build_matches_oracle_beyond_2m(bh, orc, cfg):
     scale = np.abs(com).max(1) + length
     assert np.all(np.abs(t["node4"][:, :2] - com).max(1) <= 1e-5 * scale + 1e-30)
     sim.close()
-
-
-@pytest.mark.parametrize("n,scenario,cfg", [
-    (2, "default", dict(mortonDomain="bbox", softening="plummer")),
-    (3, "default", dict(walk="group", mortonDomain="bbox", softening="plummer")),
-    (511, "two-clusters", dict(walk="group", mortonDomain="bbox", softening="plummer")),
-    (5000, "default", dict(mortonDomain="bbox", softening="plummer")),
-    (70001, "gaussian-mixture", dict(walk="group", mortonBits=64, softening="plummer",
-                                     plummerEps=1e-4)),
-    (300000, "colliding-disks", dict(walk="group", mortonDomain="bbox", softening="plummer")),
-    (300000, "default", dict(mortonDomain="fixed2000")),   # the reference's duplicate-heavy keys
-], ids=["n2", "n3", "n511", "n5000-ref-layout", "n70001-64bit", "n300k", "n300k-fixed2000"])
-@pytest.mark.parametrize("small_cap", [False, True], ids=["upper", "hand-over"])
-def test_split_build_every_size_matches_oracle(bh, orc, n, scenario, cfg, small_cap):
-    """The split build (local phase, upper levels combining the frontier
-    nodes in shared memory, device-scope climb of what they hand over) at
-    sizes where the fused build normally runs: tree arrays bit for bit
-    against the oracle.  With small_cap the upper levels combine at most 64
-    nodes per CTA, so most runs take the hand-over path (a marker in the
-    run, the device-scope climb finishing the tree)."""
-    sim = make_sim(bh, n, scenario, seed=2, **cfg)
-    flags = bh.BH_DEBUG_SPLIT_BUILD | (bh.BH_DEBUG_UPPER_CAP_SMALL if small_cap else 0)
-    sim.debugSetLimits(flags=flags)
-    bits64 = cfg.get("mortonBits") == 64
-    bbox = 1 if bits64 or cfg.get("mortonDomain") == "bbox" else 0
-    # reset, bbox, encode, sort passes, split build, walk
-    assert sim.kernels_per_step() == (1 + bbox + 1 + (8 if bits64 else 4)
-                                      + split_build_kernels(n) + 1)
-    compare_tree(orc, sim)
-    sim.close()
-
-
-@pytest.mark.parametrize("cfg", [
-    dict(walk="group", mortonDomain="bbox", softening="plummer", plummerEps=1e-3, deltaTime=1e-3),
-    dict(walk="group", mortonBits=64, softening="plummer", plummerEps=1e-4, deltaTime=1e-4,
-         integrator="leapfrog-kdk"),
-    dict(mortonDomain="bbox", softening="plummer", plummerEps=1e-3, deltaTime=1e-3),
-], ids=["group-32bit", "group-64bit-kdk", "exact-walk"])
-def test_split_build_steps_equal_fused_build(bh, cfg):
-    """Node records, and so every step, are bit-identical between the fused
-    build and the split build (same combine order and the same FP64 rule),
-    here on 200,000 bodies over 4 steps, with and without the hand-over."""
-    n = 200000
-    runs = []
-    for flags in (0, bh.BH_DEBUG_SPLIT_BUILD, bh.BH_DEBUG_SPLIT_BUILD | bh.BH_DEBUG_UPPER_CAP_SMALL):
-        sim = make_sim(bh, n, "colliding-disks", seed=9, **cfg)
-        sim.debugSetLimits(flags=flags)
-        sim.step(4)
-        m, p, v = sim.download()
-        t = sim.tree()
-        runs.append((p, v, t["node4"], t["aabb"], t["parent"]))
-        sim.close()
-    for other in runs[1:]:
-        for x, y in zip(runs[0], other):
-            assert np.array_equal(x, y)
 
 
 def test_headline_workload_tree_matches_oracle_800k(bh, orc):

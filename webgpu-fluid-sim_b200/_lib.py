@@ -30,8 +30,6 @@ BH_INTEGRATOR_LEAPFROG_KDK = 1
 BH_STAGE_NAMES = ("morton", "sort", "tree", "walk", "other")
 
 BH_DEBUG_LOOKBACK_UNPUBLISHED = 1
-BH_DEBUG_UPPER_CAP_SMALL = 2
-BH_DEBUG_SPLIT_BUILD = 4
 
 
 class bh_config(ctypes.Structure):

@@ -45,12 +45,6 @@ constexpr uint32_t kSpinCapDefault = 1u << 22;
 // Test hook: the second tile of the first sort pass waits on a predecessor
 // status that never reads as published, so its bounded wait runs out.
 constexpr uint32_t kDebugLookbackUnpublished = 1u << 0;
-// the hierarchical build's upper levels combine at most kDebugUpperCap
-// super-leaves per CTA, so larger runs take the hand-over path
-constexpr uint32_t kDebugUpperCapSmall = 1u << 1;
-constexpr uint32_t kDebugUpperCap = 64;
-// the split (local phase + upper levels) build at every body count from 2
-constexpr uint32_t kDebugSplitBuild = 1u << 2;
 
 // Packed internal-node record of the group walk (64 B, one per internal node):
 // the criterion reads `box`, an accepted node contributes `mom` + `quad`, an
@@ -179,10 +173,7 @@ struct DeviceBuffers {
     GNode* gnode = nullptr;      // n-1 packed records (group walk only; else null)
     uint2* groups = nullptr;     // n {first slot, count}: maximal subtrees of <= G bodies (group walk)
     uint32_t group_max = 0;      // G = 32 x bodies per lane (0: no groups)
-    uint2* frontier = nullptr;   // n {first slot, last slot}: nodes left to the device-scope climb
-    uint2* seg = nullptr;        // hierarchical build: per-CTA runs of frontier nodes (n + one CTA)
-    uint32_t* seg_count = nullptr;  // their lengths, every level
-    uint32_t upper_cap = 0;      // super-leaves an upper-level CTA combines (test hook: lower)
+    uint2* frontier = nullptr;   // n {first slot, last slot}: nodes left by the build's local phase
     // scratch
     StepScratch* scratch = nullptr;
     uint32_t* status = nullptr;  // look-back status: passes * tiles * 256
@@ -239,14 +230,7 @@ void launch_build_fill(const DeviceBuffers& b, int fp64_levels, cudaStream_t s);
 #define BH_SPLIT_BUILD_MIN (1u << 21)
 #endif
 constexpr uint32_t kSplitBuildMin = BH_SPLIT_BUILD_MIN;
-bool split_build(uint32_t n, uint32_t debug_flags);
-// Sizes of the hierarchical build's buffers for n bodies: run entries, run
-// lengths; and the super-leaves one upper-level CTA combines.
-size_t hier_seg_entries(uint32_t n);
-size_t hier_seg_counts(uint32_t n);
-uint32_t hier_upper_cap(uint32_t debug_flags);
-// Kernels the build launches for n bodies.
-int build_kernel_count(uint32_t n, uint32_t debug_flags);
+bool split_build(uint32_t n);
 void launch_ref_layout(const DeviceBuffers& b, cudaStream_t s);  // group walk: node4/aabb/children/range on request
 void init_bound(const DeviceBuffers& b, cudaStream_t s);
 // walk.cu

@@ -335,9 +335,6 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     size_t o_aabb = c.take<float4>(ni), o_range = c.take<uint2>(ni), o_big = c.take<double2>(2 * ni);
     size_t o_bound = c.take<uint32_t>(ni);
     size_t o_front = c.take<uint2>(nb);
-    // hierarchical build: runs of frontier nodes (a whole CTA's worth of slack)
-    // and their lengths on every level (under 2 per CTA of the local phase)
-    size_t o_seg = c.take<uint2>(bh::hier_seg_entries(n)), o_segc = c.take<uint32_t>(bh::hier_seg_counts(n));
     const bool group = s->cfg.walk_mode == BH_WALK_GROUP;
     size_t o_gnode = group ? c.take<bh::GNode>(ni) : 0;
     size_t o_groups = group ? c.take<uint2>(nb) : 0;
@@ -381,9 +378,6 @@ static int alloc_buffers(bh_sim* s, uint32_t n) {
     b.big = (double2*)(a + o_big);
     b.bound = (uint32_t*)(a + o_bound);
     b.frontier = (uint2*)(a + o_front);
-    b.seg = (uint2*)(a + o_seg);
-    b.seg_count = (uint32_t*)(a + o_segc);
-    b.upper_cap = bh::hier_upper_cap(s->debug_flags);
     b.gnode = group ? (bh::GNode*)(a + o_gnode) : nullptr;
     b.groups = group ? (uint2*)(a + o_groups) : nullptr;
     b.group_max = group ? 32u * (uint32_t)(s->cfg.bodies_per_lane > 0 ? s->cfg.bodies_per_lane : 2) : 0u;
@@ -605,7 +599,7 @@ static int check_device_errors(bh_sim* s) {
     std::string msg = "device check failed:";
     if (e & bh::kErrLookbackSpin) msg += " sort look-back gave up waiting;";
     if (e & bh::kErrStackOverflow) msg += " walk stack full (children dropped);";
-    if (e & bh::kErrTreeSpin) msg += " tree build check failed;";
+    if (e & bh::kErrTreeSpin) msg += " tree build gave up waiting;";
     if (e & bh::kErrGroupStack) msg += " group-walk stack full;";
     if (e & bh::kErrShardCapacity) msg += " shard chunk too small for its updated bodies;";
     // Restore the build's exchange slots so the next step starts clean.
@@ -1333,7 +1327,7 @@ extern "C" int bh_walk_stats(bh_sim* s, uint64_t* node_visits, uint64_t* multipo
 extern "C" int bh_debug_set_limits(bh_sim* s, uint32_t flags, uint32_t lookback_spin_cap,
                                    uint32_t walk_stack_cap) {
     BH_HANDLE(s);
-    if (flags & ~(bh::kDebugLookbackUnpublished | bh::kDebugUpperCapSmall | bh::kDebugSplitBuild))
+    if (flags & ~bh::kDebugLookbackUnpublished)
         return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_debug_set_limits: unknown flag");
     if (walk_stack_cap == 1)
         return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_debug_set_limits: a walk stack needs 2 entries");
@@ -1342,7 +1336,6 @@ extern "C" int bh_debug_set_limits(bh_sim* s, uint32_t flags, uint32_t lookback_
     s->debug_stack_cap = walk_stack_cap;
     s->b.spin_cap = lookback_spin_cap ? lookback_spin_cap : bh::kSpinCapDefault;
     s->b.debug_flags = flags;
-    s->b.upper_cap = bh::hier_upper_cap(flags);
     destroy_graphs(s);  // captured steps carry the old kernel parameters
     return BH_OK;
 }
@@ -1550,7 +1543,7 @@ extern "C" int bh_kernels_per_step(bh_sim* s, uint32_t* out) {
     if (needs_bbox(s) || s->b.num_systems) k += 1;                 // bbox (per system)
     k += 1;                                                         // encode
     k += (uint32_t)bh::sort_passes(s->b);                          // sort passes
-    k += bh::build_kernel_count(s->b.n, s->b.debug_flags);                            // build + fill (+ upper levels, climb)
+    k += bh::split_build(s->b.n) ? 2 : 1;                           // build + fill (+ frontier climb)
     k += 1;                                                         // walk + integrate
     *out = s->b.n ? k : 0;
     return BH_OK;

@@ -1,44 +1,18 @@
-// tree.cu -- launches the hierarchy build + fill for the engine's step: below
-// kSplitBuildMin bodies one fused kernel; from there the block-local phase
-// (build_fill_kernel<K, true>), the upper levels over its frontier nodes
-// (build_upper_kernel, until one CTA holds the whole run) and the
-// device-scope climb of whatever they leave (build_climb_kernel, normally
-// nothing).  The kernels and their derivation are in tree_kernel.cuh.
+// tree.cu -- launches the hierarchy build + fill for the engine's step: the
+// block-local phase (build_fill_kernel<K, true>) and the climb of the
+// frontier nodes it leaves (build_climb_kernel).  The kernels and their
+// derivation are in tree_kernel.cuh.
 #include "tree_kernel.cuh"
 
 namespace bh {
 
-bool split_build(uint32_t n, uint32_t debug_flags) {
-    return n >= kSplitBuildMin || (n >= 2 && (debug_flags & kDebugSplitBuild));
-}
-
-static uint32_t local_ctas(uint32_t n) { return (n + kBuildBlockSplit - 1) / kBuildBlockSplit; }
-
-// Upper levels after a local phase of `ctas` CTAs (the last one is a single CTA).
-static int upper_levels(uint32_t ctas) {
-    int k = 0;
-    for (uint32_t c = ctas; c > 1; c = (c + kUpperSegs - 1) / kUpperSegs) ++k;
-    return k;
-}
-
-size_t hier_seg_entries(uint32_t n) { return (size_t)local_ctas(n ? n : 1) * kBuildBlockSplit; }
-size_t hier_seg_counts(uint32_t n) { return 2 * (size_t)local_ctas(n ? n : 1) + 64; }
-uint32_t hier_upper_cap(uint32_t debug_flags) {
-    return (debug_flags & kDebugUpperCapSmall) ? kDebugUpperCap : (uint32_t)kUpperCap;
-}
-int build_kernel_count(uint32_t n, uint32_t debug_flags) {
-    if (!split_build(n, debug_flags)) return 1;
-    return 2 + upper_levels(local_ctas(n));
-}
+bool split_build(uint32_t n) { return n >= kSplitBuildMin; }
 
 template <typename K, bool SPLIT>
 static cudaError_t set_build_attributes() {
-    cudaError_t e = cudaFuncSetAttribute(build_fill_kernel<K, SPLIT>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(BuildShared<K, build_block<SPLIT>()>));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(build_upper_kernel<K, SPLIT>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(UpperShared));
+    return cudaFuncSetAttribute(build_fill_kernel<K, SPLIT>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(BuildShared<K, build_block<SPLIT>()>));
 }
 
 // Allow the build kernels their shared memory (dynamic; once per device,
@@ -77,36 +51,18 @@ static void launch_typed(const DeviceBuffers& b, int fp64_levels, cudaStream_t s
     a.gmax = b.group_max;
     a.xm = b.xm;
     a.err = b.err;
-    if (!split_build(b.n, b.debug_flags)) {
+    if (!split_build(b.n)) {
         constexpr uint32_t B = build_block<false>();
         build_fill_kernel<K, false><<<(b.n + B - 1) / B, B, sizeof(BuildShared<K, B>), s>>>(a);
         return;
     }
     a.frontier = b.frontier;
     a.frontier_count = &b.scratch->frontier_ctr;
-    a.seg = b.seg;
-    a.seg_count = b.seg_count;
     constexpr uint32_t B = build_block<true>();
-    const uint32_t grid = local_ctas(b.n);
+    const uint32_t grid = (b.n + B - 1) / B;
     build_fill_kernel<K, true><<<grid, B, sizeof(BuildShared<K, B>), s>>>(a);
-    // Upper levels: each CTA combines the runs of kUpperSegs CTAs below.
-    uint32_t runs = grid;
-    size_t run_cap = B;
-    uint32_t* lengths = b.seg_count;
-    while (runs > 1) {
-        const uint32_t ctas = (runs + kUpperSegs - 1) / kUpperSegs;
-        if (ctas == 1)
-            build_upper_kernel<K, true><<<1, kUpperThreads, sizeof(UpperShared), s>>>(
-                a, b.seg, run_cap, lengths, runs, nullptr, b.upper_cap);
-        else
-            build_upper_kernel<K, false><<<ctas, kUpperThreads, sizeof(UpperShared), s>>>(
-                a, b.seg, run_cap, lengths, runs, lengths + runs, b.upper_cap);
-        lengths += runs;
-        run_cap *= kUpperSegs;
-        runs = ctas;
-    }
-    // Whatever the upper levels handed over (normally nothing): only the
-    // device knows how many, so a resident grid strides over them.
+    // Frontier nodes number far fewer than bodies (a handful per CTA), but
+    // only the device knows how many: a resident grid strides over them.
     static int blocks_per_sm[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);

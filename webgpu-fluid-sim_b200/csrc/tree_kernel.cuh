@@ -94,11 +94,6 @@ struct BuildArgs {
     // slot, last slot}, and their count (zero before the local phase).
     uint2* frontier = nullptr;
     unsigned int* frontier_count = nullptr;
-    // Hierarchical build: the local phase lists each CTA's frontier nodes in
-    // slot order in seg[cta * B ...] with their number in seg_count[cta]; the
-    // upper levels (build_upper_kernel) combine them.
-    uint2* seg = nullptr;
-    uint32_t* seg_count = nullptr;
     // {x, y, m, 0} per body in original order, when the encode wrote them:
     // one gather per slot instead of a position and a mass
     const float4* xm = nullptr;
@@ -152,7 +147,6 @@ struct BuildShared {
     uint32_t bound[B + 1];  // exchange slots of the local splits
     float leaf[3][B];       // leaf {m, x, y} by slot - B0
     float rec[10][B];       // local internal node {m, cx, cy, box, S} by index - B0
-    uint32_t fr[B];         // split build: last slot of the frontier node starting at slot B0 + q
 };
 
 // The node a climbing thread currently owns: its slot range, the deltas at
@@ -192,9 +186,8 @@ __device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, Buil
             c.local = local;
         }
         if (STOP && !local) {
-            // The parent split lies outside this CTA: the node is one of the
-            // CTA's frontier nodes, listed in slot order when the CTA is done.
-            S->fr[c.l - B0] = c.r;
+            // The parent split lies outside this CTA: leave it to the climb kernel.
+            A.frontier[atomicAdd(A.frontier_count, 1u)] = make_uint2(c.l, c.r);
             return false;
         }
         // Past the stop test a split build's first kernel is always local;
@@ -431,7 +424,6 @@ build_fill_kernel(const BuildArgs<K> A) {
         S.key[q] = (g >= 0 && g < (long long)n) ? __ldg(&A.keys[g]) : (K)0;
     }
     for (int q = t; q <= B; q += B) S.bound[q] = kSentinel;
-    if (SPLIT) S.fr[t] = kSentinel;  // before the barriers that precede every climb
     __syncthreads();
     for (int q = t; q <= B; q += B) {
         const long long g = (long long)B0 - 1 + q;
@@ -468,64 +460,45 @@ build_fill_kernel(const BuildArgs<K> A) {
         }
         __syncthreads();
     }
-    if (i < n) {
-        const uint32_t body = __ldg(&A.ids[i]);
-        float m;
-        float2 p;
-        if (A.xm) {
-            const float4 r = __ldg(&A.xm[body]);
-            m = r.z;
-            p = make_float2(r.x, r.y);
-        } else {
-            m = __ldg(&A.mass[body]);
-            p = __ldg(&A.pos[body]);
-        }
-        A.node4[nm1 + i] = make_float4(p.x, p.y, m, 0.0f);  // leaf (lbvh.wgsl:179-187)
-        S.leaf[0][t] = m;
-        S.leaf[1][t] = p.x;
-        S.leaf[2][t] = p.y;
-        Climb c;
-        c.l = i;
-        c.r = i;
-        // delta at the two boundaries of the current range (-1 outside [0, n-1]);
-        // a parent keeps one of them, so each level computes only one new delta.
-        c.dl = S.d[t];
-        c.dr = S.d[t + 1];
-        c.cm = m; c.cx = p.x; c.cy = p.y;
-        c.lox = p.x; c.loy = p.y; c.hix = p.x; c.hiy = p.y;
-        c.sxx = 0.0f; c.sxy = 0.0f; c.syy = 0.0f;
-        c.dm = 0.0; c.dmx = 0.0; c.dmy = 0.0;
-        c.local = true;
-        climb<K, B, true, SPLIT>(A, c, &S, B0);
+    if (i >= n) return;
+
+    const uint32_t body = __ldg(&A.ids[i]);
+    float m;
+    float2 p;
+    if (A.xm) {
+        const float4 r = __ldg(&A.xm[body]);
+        m = r.z;
+        p = make_float2(r.x, r.y);
+    } else {
+        m = __ldg(&A.mass[body]);
+        p = __ldg(&A.pos[body]);
     }
-    if (SPLIT) {
-        // The CTA's frontier nodes partition its slots: list them in slot
-        // order (a ballot and a scan over the first slots) for the upper levels.
-        __syncthreads();
-        const uint32_t r = S.fr[t];
-        const bool f = r != kSentinel;
-        const unsigned ballot = __ballot_sync(0xFFFFFFFFu, f);
-        if (lane == 0) S.wmin[0][warp] = __popc(ballot);
-        __syncthreads();
-        uint32_t off = __popc(ballot & ((1u << lane) - 1u)), total = 0;
-#pragma unroll
-        for (int w = 0; w < B / 32; ++w) {
-            const uint32_t cw = (uint32_t)S.wmin[0][w];
-            off += (w < warp) ? cw : 0u;
-            total += cw;
-        }
-        if (f) A.seg[(size_t)blockIdx.x * B + off] = make_uint2(B0 + (uint32_t)t, r);
-        if (t == 0) A.seg_count[blockIdx.x] = total;
-    }
+    A.node4[nm1 + i] = make_float4(p.x, p.y, m, 0.0f);  // leaf (lbvh.wgsl:179-187)
+    S.leaf[0][t] = m;
+    S.leaf[1][t] = p.x;
+    S.leaf[2][t] = p.y;
+    Climb c;
+    c.l = i;
+    c.r = i;
+    // delta at the two boundaries of the current range (-1 outside [0, n-1]);
+    // a parent keeps one of them, so each level computes only one new delta.
+    c.dl = S.d[t];
+    c.dr = S.d[t + 1];
+    c.cm = m; c.cx = p.x; c.cy = p.y;
+    c.lox = p.x; c.loy = p.y; c.hix = p.x; c.hiy = p.y;
+    c.sxx = 0.0f; c.sxy = 0.0f; c.syy = 0.0f;
+    c.dm = 0.0; c.dmx = 0.0; c.dmy = 0.0;
+    c.local = true;
+    climb<K, B, true, SPLIT>(A, c, &S, B0);
 }
 
-// Last kernel of the split build: one thread per frontier node left by the
-// kernels before (a node made by them, or a leaf, whose parent split they
-// could not combine) continues the climb with the device-scope protocol.
-// The node's record is read back from the tree arrays the earlier kernels
-// wrote, with its FP64 sums when it has kFp64MinBodies bodies or more.  Each
-// climb ends without waiting for any other thread, so a thread may take
-// several entries.
+// Second kernel of the split build: one thread per frontier node (a node
+// made in the local phase, or a leaf, whose parent split is outside its
+// CTA) continues the climb with the device-scope protocol.  The node's
+// record is read back from the tree arrays the first kernel wrote; no
+// frontier node is large enough for the FP64 path (local nodes hold fewer
+// than kBuildBlockSplit < kFp64MinBodies bodies).  Each climb ends without
+// waiting for any other thread, so a thread may take several entries.
 template <typename K>
 __global__ void __launch_bounds__(kClimbBlock)
 build_climb_kernel(const BuildArgs<K> A) {
@@ -561,475 +534,8 @@ build_climb_kernel(const BuildArgs<K> A) {
             }
             c.cm = mom.z; c.cx = mom.x; c.cy = mom.y;
             c.lox = box.x; c.loy = box.y; c.hix = box.z; c.hiy = box.w;
-            if (A.fp64 && c.r - c.l + 1 >= kFp64MinBodies) {
-                const double2 b0 = __ldcg(&A.big[2 * (size_t)idx]);
-                const double2 b1 = __ldcg(&A.big[2 * (size_t)idx + 1]);
-                c.dm = b0.x; c.dmx = b0.y; c.dmy = b1.x;
-            }
         }
         climb<K, kBuildBlockSplit, false, false>(A, c, nullptr, 0u);
-    }
-}
-
-
-// ---- upper levels of the hierarchical build ---------------------------------
-//
-// The local phase leaves, per CTA, its frontier nodes in slot order.  Those
-// of kUpperSegs consecutive CTAs partition a run of slots, and the nodes
-// above them form the same kind of tree over fewer "super-leaves": the
-// hierarchy is the Cartesian tree of the boundary deltas, and every boundary
-// inside a super-leaf is irrelevant above it.  One CTA of build_upper_kernel
-// takes such a run (up to kUpperCap super-leaves), applies the local test of
-// the local phase to the deltas at the boundaries between super-leaves, and
-// climbs from every super-leaf with the same agglomerative rule, exchanging
-// through shared memory: the climbs that took dozens of device-scope round
-// trips in the frontier climb take shared-memory ones here.  Nodes whose
-// parent split is not local are the next level's super-leaves, again listed
-// in slot order (written over the CTA's own input).  A level whose runs all
-// fit one CTA reaches the root.  Records and node numbering are those of the
-// local phase (Karras index = range end next to the parent's split).
-//
-// A run of more than kUpperCap super-leaves (a degenerate tree) is handed
-// whole to the device-scope climb and replaced by one marker entry; a CTA
-// that sees a marker passes its run on unchanged, so no node is ever
-// combined across bodies the CTA does not hold.  The last level passes
-// whatever it could not combine to build_climb_kernel (normally nothing).
-constexpr int kUpperThreads = 1024;
-constexpr int kUpperCap = 2048;   // super-leaves one CTA combines
-constexpr int kUpperSegs = 128;   // input runs (CTAs of the level below) per CTA
-constexpr uint32_t kUpperMarker = 0xFFFFFFFFu;
-
-struct UpperShared {
-    uint2 sl[kUpperCap];            // super-leaves {first slot, last slot}, in slot order
-    int d[kUpperCap + 1];           // delta at boundary q, between super-leaves q-1 and q
-    uint32_t bound[kUpperCap + 1];  // exchange slots of the local splits
-    uint32_t fr[kUpperCap];         // last super-leaf of the frontier node starting at q
-    float rec[10][kUpperCap];       // records {m, cx, cy, box, S} by compact index
-    double big[3][kUpperCap];       // their FP64 {m, m x, m y} (>= kFp64MinBodies bodies)
-    uint32_t link[4][kUpperCap];    // nodes made here: left, right, first slot, count | side bit
-    unsigned char made[kUpperCap];  // a node made here is stored under this index
-    uint32_t seg_off[kUpperSegs];
-    int wmin[2][kUpperThreads / 32];
-    uint32_t wcnt[kUpperThreads / 32];
-    uint32_t total, marker;
-    unsigned char local[kUpperCap + 1];
-};
-
-// A climb over super-leaves: compact range [a, b], slot range [l, r].
-struct UpperClimb {
-    uint32_t a, b, l, r;
-    int dl, dr;
-    float cm, cx, cy;
-    float lox, loy, hix, hiy;
-    float sxx, sxy, syy;
-    double dm, dmx, dmy;
-};
-
-// One level of an upper climb (see climb_step for the record arithmetic).
-// A node made here is stored in shared memory under its compact Karras end:
-// its last super-leaf when it is a left child, its first when a right child
-// (two nodes of two or more super-leaves never share that index).
-template <typename K>
-__device__ __forceinline__ bool upper_step(const BuildArgs<K>& A, UpperClimb& c, UpperShared& S,
-                                        uint32_t m) {
-    const uint32_t n = A.n, nm1 = n - 1;
-    const bool is_left = c.dr > c.dl;
-    const uint32_t gamma = is_left ? c.r : c.l - 1;
-    const uint32_t qb = is_left ? c.b + 1 : c.a;  // the split's boundary, compact
-    if (qb < 1 || qb > m - 1 || !S.local[qb]) {
-        S.fr[c.a] = c.b;  // a super-leaf of the next level
-        return false;
-    }
-    __threadfence_block();
-    const uint32_t other = atomicExch(&S.bound[qb], is_left ? c.a : c.b);
-    if (other == kSentinel) return false;  // first to arrive: the sibling's thread goes on
-    __threadfence_block();
-    const uint32_t pa = is_left ? c.a : other, pb = is_left ? other : c.b;
-    if (pa >= m || pb >= m || pa > pb) {  // cannot happen; never index outside the run
-        if (A.err) atomicOr(const_cast<uint32_t*>(A.err), kErrTreeSpin);
-        return false;
-    }
-    const uint32_t pl = S.sl[pa].x, pr = S.sl[pb].y;
-    const uint32_t li = (pl == gamma) ? nm1 + gamma : gamma;
-    const uint32_t ri = (pr == gamma + 1) ? nm1 + gamma + 1 : gamma + 1;
-    const uint32_t sib_cnt = is_left ? (pr - gamma) : (gamma - pl + 1);
-    const uint32_t sa = is_left ? c.b + 1 : pa, sz = is_left ? pb : c.a - 1;
-    const uint32_t my_cnt = c.r - c.l + 1;
-    const uint32_t cnt = pr - pl + 1;
-    // The sibling's record is in shared memory: a super-leaf's since the
-    // start (under its own index), a node made here under its compact Karras
-    // end (a right child's first super-leaf, a left child's last), which for
-    // a one-super-leaf sibling is the same index.
-    const uint32_t k = is_left ? sa : sz;
-    volatile float* vr = &S.rec[0][0];
-    const float4 s4 = make_float4(vr[kUpperCap + k], vr[2 * kUpperCap + k], vr[k], 0.f);
-    const float4 sb = make_float4(vr[3 * kUpperCap + k], vr[4 * kUpperCap + k],
-                                  vr[5 * kUpperCap + k], vr[6 * kUpperCap + k]);
-    const float4 sq = make_float4(vr[7 * kUpperCap + k], vr[8 * kUpperCap + k],
-                                  vr[9 * kUpperCap + k], 0.f);
-    double sm = 0.0, smx = 0.0, smy = 0.0;
-    if (A.fp64 && sib_cnt >= kFp64MinBodies) {
-        volatile double* vb = &S.big[0][0];
-        sm = vb[k]; smx = vb[kUpperCap + k]; smy = vb[2 * kUpperCap + k];
-    }
-    if (A.fp64 && sib_cnt < kFp64MinBodies) {
-        sm = (double)s4.z; smx = (double)s4.z * (double)s4.x; smy = (double)s4.z * (double)s4.y;
-    }
-    c.lox = fminf(c.lox, sb.x);
-    c.loy = fminf(c.loy, sb.y);
-    c.hix = fmaxf(c.hix, sb.z);
-    c.hiy = fmaxf(c.hiy, sb.w);
-    const int dpl = is_left ? c.dl : S.d[pa];
-    const int dpr = is_left ? S.d[pb + 1] : c.dr;
-    float tm, ncx, ncy;
-    const bool big = A.fp64 && cnt >= kFp64MinBodies;
-    if (big) {
-        if (my_cnt < kFp64MinBodies) {
-            c.dm = (double)c.cm; c.dmx = (double)c.cm * (double)c.cx; c.dmy = (double)c.cm * (double)c.cy;
-        }
-        c.dm += sm;
-        c.dmx += smx;
-        c.dmy += smy;
-        tm = (float)c.dm;
-        ncx = c.dm > 0.0 ? (float)(c.dmx / c.dm) : 0.0f;
-        ncy = c.dm > 0.0 ? (float)(c.dmy / c.dm) : 0.0f;
-    } else {
-        float ml, mr, clx, cly, crx, cry;
-        if (is_left) { ml = c.cm; clx = c.cx; cly = c.cy; mr = s4.z; crx = s4.x; cry = s4.y; }
-        else { ml = s4.z; clx = s4.x; cly = s4.y; mr = c.cm; crx = c.cx; cry = c.cy; }
-        tm = __fadd_rn(ml, mr);
-        if (tm > 0.0f) {
-            ncx = __fdiv_rn(__fadd_rn(__fmul_rn(clx, ml), __fmul_rn(crx, mr)), tm);
-            ncy = __fdiv_rn(__fadd_rn(__fmul_rn(cly, ml), __fmul_rn(cry, mr)), tm);
-        } else {
-            ncx = 0.0f;
-            ncy = 0.0f;
-        }
-    }
-    if (A.gnode) {
-        float ml, mr, lxx, lxy, lyy, rxx, rxy, ryy, dlx, dly, drx, dry;
-        if (is_left) {
-            ml = c.cm; lxx = c.sxx; lxy = c.sxy; lyy = c.syy; dlx = __fsub_rn(c.cx, ncx); dly = __fsub_rn(c.cy, ncy);
-            mr = s4.z; rxx = sq.x; rxy = sq.y; ryy = sq.z; drx = __fsub_rn(s4.x, ncx); dry = __fsub_rn(s4.y, ncy);
-        } else {
-            ml = s4.z; lxx = sq.x; lxy = sq.y; lyy = sq.z; dlx = __fsub_rn(s4.x, ncx); dly = __fsub_rn(s4.y, ncy);
-            mr = c.cm; rxx = c.sxx; rxy = c.sxy; ryy = c.syy; drx = __fsub_rn(c.cx, ncx); dry = __fsub_rn(c.cy, ncy);
-        }
-        c.sxx = __fadd_rn(__fadd_rn(lxx, __fmul_rn(ml, __fmul_rn(dlx, dlx))),
-                          __fadd_rn(rxx, __fmul_rn(mr, __fmul_rn(drx, drx))));
-        c.sxy = __fadd_rn(__fadd_rn(lxy, __fmul_rn(ml, __fmul_rn(dlx, dly))),
-                          __fadd_rn(rxy, __fmul_rn(mr, __fmul_rn(drx, dry))));
-        c.syy = __fadd_rn(__fadd_rn(lyy, __fmul_rn(ml, __fmul_rn(dly, dly))),
-                          __fadd_rn(ryy, __fmul_rn(mr, __fmul_rn(dry, dry))));
-    }
-    {
-        // The record goes to shared memory only (the tree arrays are written
-        // after the climbs, so no fence here waits on global stores); the
-        // root is stored under its first super-leaf like any other left end.
-        const bool right_end = dpr > dpl;
-        const uint32_t k = right_end ? pb : pa;
-        volatile float* vr = &S.rec[0][0];
-        vr[k] = tm;
-        vr[kUpperCap + k] = ncx;
-        vr[2 * kUpperCap + k] = ncy;
-        vr[3 * kUpperCap + k] = c.lox;
-        vr[4 * kUpperCap + k] = c.loy;
-        vr[5 * kUpperCap + k] = c.hix;
-        vr[6 * kUpperCap + k] = c.hiy;
-        vr[7 * kUpperCap + k] = c.sxx;
-        vr[8 * kUpperCap + k] = c.sxy;
-        vr[9 * kUpperCap + k] = c.syy;
-        if (big) {
-            volatile double* vb = &S.big[0][0];
-            vb[k] = c.dm;
-            vb[kUpperCap + k] = c.dmx;
-            vb[2 * kUpperCap + k] = c.dmy;
-        }
-        S.link[0][k] = li;
-        S.link[1][k] = ri;
-        S.link[2][k] = pl;
-        S.link[3][k] = cnt | (right_end ? 0x80000000u : 0u);
-        S.made[k] = 1;
-        if (pl == 0 && pr == nm1) return false;  // the root
-    }
-    c.cm = tm; c.cx = ncx; c.cy = ncy;
-    c.a = pa; c.b = pb;
-    c.l = pl; c.r = pr;
-    c.dl = dpl; c.dr = dpr;
-    return true;
-}
-
-// Block-wide exclusive sum over threads (every thread takes part).
-__device__ __forceinline__ uint32_t upper_excl_sum(uint32_t v, uint32_t* wcnt, uint32_t* total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) wcnt[warp] = x;
-    __syncthreads();
-    uint32_t before = 0, all = 0;
-    for (int w = 0; w < kUpperThreads / 32; ++w) {
-        const uint32_t cw = wcnt[w];
-        before += (w < warp) ? cw : 0u;
-        all += cw;
-    }
-    __syncthreads();
-    *total = all;
-    return before + x - v;
-}
-
-// One level of the upper build.  Input: in_segs runs, run s holding
-// in_count[s] super-leaves at seg[s * in_cap ...].  CTA c takes runs
-// [c kUpperSegs, (c+1) kUpperSegs) and writes the next level's run over the
-// start of its own input, with its length in out_count[c]; with FLAT (the
-// last level, one CTA) what remains goes to the device-scope climb's list.
-template <typename K, bool FLAT>
-__global__ void __launch_bounds__(kUpperThreads, 1)
-build_upper_kernel(const BuildArgs<K> A, uint2* __restrict__ seg, size_t in_cap,
-                   const uint32_t* __restrict__ in_count, uint32_t in_segs,
-                   uint32_t* __restrict__ out_count, uint32_t cap_limit) {
-    extern __shared__ __align__(16) unsigned char upper_smem[];
-    UpperShared& S = *reinterpret_cast<UpperShared*>(upper_smem);
-    if (step_failed(A.err)) return;  // uniform over the block
-    const int t = (int)threadIdx.x;
-    const uint32_t n = A.n, nm1 = n - 1;
-    const uint32_t s0 = blockIdx.x * (uint32_t)kUpperSegs;
-    const uint32_t nseg = min((uint32_t)kUpperSegs, in_segs - s0);
-    uint2* region = seg + (size_t)s0 * in_cap;
-    const uint32_t cnt = (t < (int)nseg) ? in_count[s0 + t] : 0u;
-    uint32_t m;
-    const uint32_t off = upper_excl_sum(cnt, S.wcnt, &m);
-    if (t < kUpperSegs) S.seg_off[t] = off;
-    if (t == 0) S.marker = 0;
-    __syncthreads();
-    const auto to_climb = [&](uint2 e) {
-        if (e.x != kUpperMarker) A.frontier[atomicAdd(A.frontier_count, 1u)] = e;
-    };
-    if (m > cap_limit) {
-        // Too many super-leaves for one CTA: the device-scope climb takes them all.
-        if (t < (int)nseg)
-            for (uint32_t k = 0; k < cnt; ++k) to_climb(region[(size_t)t * in_cap + k]);
-        __syncthreads();  // every entry read before the run is overwritten
-        if (!FLAT && t == 0) {
-            region[0] = make_uint2(kUpperMarker, kUpperMarker);
-            out_count[blockIdx.x] = 1u;
-        }
-        return;
-    }
-    // The runs' entries in order, every load in flight at once: entry j
-    // belongs to the last run whose offset is <= j.
-    for (uint32_t j = (uint32_t)t; j < m; j += kUpperThreads) {
-        uint32_t lo = 0, hi = nseg - 1;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1) >> 1;
-            if (S.seg_off[mid] <= j) lo = mid;
-            else hi = mid - 1;
-        }
-        const uint2 e = region[(size_t)lo * in_cap + (j - S.seg_off[lo])];
-        S.sl[j] = e;
-        if (e.x == kUpperMarker) S.marker = 1u;
-    }
-    __syncthreads();
-    if (S.marker || m < 2) {
-        // A run with a hole (or nothing to combine): passed on unchanged.
-        for (uint32_t j = (uint32_t)t; j < m; j += kUpperThreads) {
-            if (FLAT) to_climb(S.sl[j]);
-            else region[j] = S.sl[j];
-        }
-        if (!FLAT && t == 0) out_count[blockIdx.x] = m;
-        return;
-    }
-    // Deltas at the boundaries between super-leaves (and at the run's ends).
-    for (uint32_t q = (uint32_t)t; q <= m; q += kUpperThreads) {
-        const long long g = (q < m) ? (long long)S.sl[q].x - 1 : (long long)S.sl[m - 1].y;
-        S.d[q] = (g < 0 || g >= (long long)nm1) ? -1 : delta_at(A.keys, (uint32_t)g, (uint32_t)g + 1u);
-        S.bound[q] = kSentinel;
-        if (q < m) {
-            S.fr[q] = kSentinel;
-            S.made[q] = 0;
-        }
-    }
-    __syncthreads();
-    // Local splits: a smaller delta among the run's boundaries on both sides.
-    // Thread t owns boundaries [t P, (t+1) P) with P = 2 (m + 1 <= 2049
-    // boundaries; the last thread also takes q = 2048).
-    {
-        constexpr int P = (kUpperCap + kUpperThreads - 1) / kUpperThreads;
-        static_assert(P == 2, "two boundaries per thread");
-        const int lane = t & 31, warp = t >> 5;
-        const int q0 = t * P;
-        const int INF = 0x7FFFFFFF;
-        int v[P + 1];
-#pragma unroll
-        for (int k = 0; k <= P; ++k) {
-            const int q = q0 + k;
-            v[k] = (q <= (int)m && (k < P || t == kUpperThreads - 1)) ? S.d[q] : INF;
-        }
-        int cmin = min(v[0], v[1]);
-        if (t == kUpperThreads - 1) cmin = min(cmin, v[2]);
-        // exclusive prefix minimum and exclusive suffix minimum of the chunk minima
-        int pm = cmin, sm = cmin;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int a = __shfl_up_sync(0xFFFFFFFFu, pm, o);
-            const int b = __shfl_down_sync(0xFFFFFFFFu, sm, o);
-            if (lane >= o) pm = min(pm, a);
-            if (lane + o < 32) sm = min(sm, b);
-        }
-        if (lane == 31) S.wmin[0][warp] = pm;
-        if (lane == 0) S.wmin[1][warp] = sm;
-        __syncthreads();
-        int before = INF, after = INF;
-        for (int w = 0; w < warp; ++w) before = min(before, S.wmin[0][w]);
-        for (int w = warp + 1; w < kUpperThreads / 32; ++w) after = min(after, S.wmin[1][w]);
-        const int pprev = __shfl_up_sync(0xFFFFFFFFu, pm, 1);
-        const int snext = __shfl_down_sync(0xFFFFFFFFu, sm, 1);
-        int left = min(before, lane > 0 ? pprev : INF);     // min over boundaries < q0
-        int right = min(after, lane < 31 ? snext : INF);    // min over boundaries >= q0 + P (other threads)
-        // suffix minima inside the chunk, then the flags
-        int suf[P + 1];
-        suf[P] = (t == kUpperThreads - 1) ? min(v[P], right) : right;
-        for (int k = P - 1; k >= 0; --k) suf[k] = min(v[k], suf[k + 1]);
-#pragma unroll
-        for (int k = 0; k <= P; ++k) {
-            const int q = q0 + k;
-            if (k == P && t != kUpperThreads - 1) break;
-            if (q > (int)m) break;
-            const bool loc = q >= 1 && q <= (int)m - 1 && left < v[k] && suf[k + 1 <= P ? k + 1 : P] < v[k];
-            S.local[q] = loc ? 1 : 0;
-            left = min(left, v[k]);
-        }
-    }
-    __syncthreads();
-    // Every super-leaf's record into shared memory, all loads in flight at
-    // once.  A super-leaf's slot is reused only by a node made here that
-    // contains it, after the super-leaf has been read.
-    for (uint32_t j = (uint32_t)t; j < m; j += kUpperThreads) {
-        const uint2 e = S.sl[j];
-        float4 box, mom, q = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (e.x == e.y) {
-            mom = __ldcg(&A.node4[nm1 + e.x]);
-            box = make_float4(mom.x, mom.y, mom.x, mom.y);
-        } else {
-            const uint32_t idx = (S.d[j + 1] > S.d[j]) ? e.y : e.x;  // Karras index
-            if (A.gnode) {
-                box = __ldcg(&A.gnode[idx].box);
-                mom = __ldcg(&A.gnode[idx].mom);
-                q = __ldcg(&A.gnode[idx].quad);
-            } else {
-                box = __ldcg(&A.aabb[idx]);
-                mom = __ldcg(&A.node4[idx]);
-            }
-            if (A.fp64 && e.y - e.x + 1 >= kFp64MinBodies) {
-                const double2 b0 = __ldcg(&A.big[2 * (size_t)idx]);
-                const double2 b1 = __ldcg(&A.big[2 * (size_t)idx + 1]);
-                S.big[0][j] = b0.x;
-                S.big[1][j] = b0.y;
-                S.big[2][j] = b1.x;
-            }
-        }
-        S.rec[0][j] = mom.z;
-        S.rec[1][j] = mom.x;
-        S.rec[2][j] = mom.y;
-        S.rec[3][j] = box.x;
-        S.rec[4][j] = box.y;
-        S.rec[5][j] = box.z;
-        S.rec[6][j] = box.w;
-        S.rec[7][j] = q.x;
-        S.rec[8][j] = q.y;
-        S.rec[9][j] = q.z;
-    }
-    __syncthreads();
-    // Climb from every super-leaf (a thread takes the next one when its climb ends).
-    for (uint32_t j = (uint32_t)t; j < m; j += kUpperThreads) {
-        UpperClimb c;
-        const uint2 e = S.sl[j];
-        c.a = j; c.b = j; c.l = e.x; c.r = e.y;
-        c.dl = S.d[j];
-        c.dr = S.d[j + 1];
-        c.cm = S.rec[0][j]; c.cx = S.rec[1][j]; c.cy = S.rec[2][j];
-        c.lox = S.rec[3][j]; c.loy = S.rec[4][j]; c.hix = S.rec[5][j]; c.hiy = S.rec[6][j];
-        c.sxx = S.rec[7][j]; c.sxy = S.rec[8][j]; c.syy = S.rec[9][j];
-        c.dm = 0.0; c.dmx = 0.0; c.dmy = 0.0;
-        if (A.fp64 && e.y - e.x + 1 >= kFp64MinBodies) {
-            c.dm = S.big[0][j]; c.dmx = S.big[1][j]; c.dmy = S.big[2][j];
-        }
-        // Every level widens the range, so a climb takes fewer than m levels.
-        for (uint32_t lv = 0; upper_step<K>(A, c, S, m); ++lv)
-            if (lv >= m) {
-                if (A.err) atomicOr(const_cast<uint32_t*>(A.err), kErrTreeSpin);
-                break;
-            }
-    }
-    __syncthreads();
-    // The nodes made here into the tree arrays (their Karras index: the
-    // range end next to the parent's split), with parents and walk groups.
-    for (uint32_t k = (uint32_t)t; k < m; k += kUpperThreads) {
-        if (!S.made[k]) continue;
-        const uint32_t li = S.link[0][k], ri = S.link[1][k], pl = S.link[2][k];
-        const uint32_t cnt = S.link[3][k] & 0x7FFFFFFFu;
-        const uint32_t pr = pl + cnt - 1;
-        const uint32_t pidx = (pl == 0 && pr == nm1) ? 0u : ((S.link[3][k] >> 31) ? pr : pl);
-        const uint32_t gamma = li >= nm1 ? li - nm1 : li;
-        const float4 box = make_float4(S.rec[3][k], S.rec[4][k], S.rec[5][k], S.rec[6][k]);
-        const float len = fmaxf(__fsub_rn(box.z, box.x), __fsub_rn(box.w, box.y));
-        const float4 mom = make_float4(S.rec[1][k], S.rec[2][k], S.rec[0][k], len);
-        if (A.gnode) {
-            GNode g;
-            g.box = box;
-            g.mom = mom;
-            g.quad = make_float4(S.rec[7][k], S.rec[8][k], S.rec[9][k], 0.0f);
-            g.link = make_uint4(li, ri, pl, cnt);
-            A.gnode[pidx] = g;
-        } else {
-            A.node4[pidx] = mom;
-            A.aabb[pidx] = box;
-            A.children[pidx] = make_uint2(li, ri);
-            A.range[pidx] = make_uint2(pl, pr);
-        }
-        if (A.fp64 && cnt >= kFp64MinBodies) {
-            A.big[2 * (size_t)pidx] = make_double2(S.big[0][k], S.big[1][k]);
-            A.big[2 * (size_t)pidx + 1] = make_double2(S.big[2][k], 0.0);
-        }
-        A.parent[li] = pidx;
-        A.parent[ri] = pidx;
-        if (pidx == 0) A.parent[0] = kSentinel;  // lbvh.wgsl:159-161
-        if (A.groups) {
-            // Walk groups: maximal subtrees of <= gmax bodies.
-            if (cnt > A.gmax) {
-                const uint32_t lcnt = gamma - pl + 1, rcnt = pr - gamma;
-                if (lcnt <= A.gmax) A.groups[atomicAdd(A.group_count, 1u)] = make_uint2(pl, lcnt);
-                if (rcnt <= A.gmax) A.groups[atomicAdd(A.group_count, 1u)] = make_uint2(gamma + 1, rcnt);
-            } else if (pidx == 0) {
-                A.groups[atomicAdd(A.group_count, 1u)] = make_uint2(0u, n);
-            }
-        }
-    }
-    // The next level's super-leaves, in slot order (each thread lists P of them).
-    {
-        constexpr int P = (kUpperCap + kUpperThreads - 1) / kUpperThreads;
-        uint32_t mine = 0;
-#pragma unroll
-        for (int k = 0; k < P; ++k) {
-            const uint32_t j = (uint32_t)t * P + k;
-            mine += (j < m && S.fr[j] != kSentinel) ? 1u : 0u;
-        }
-        uint32_t total;
-        uint32_t pos = upper_excl_sum(mine, S.wcnt, &total);
-#pragma unroll
-        for (int k = 0; k < P; ++k) {
-            const uint32_t j = (uint32_t)t * P + k;
-            if (j < m && S.fr[j] != kSentinel) {
-                const uint2 e = make_uint2(S.sl[j].x, S.sl[S.fr[j]].y);
-                if (FLAT) to_climb(e);
-                else region[pos] = e;
-                ++pos;
-            }
-        }
-        if (!FLAT && t == 0) out_count[blockIdx.x] = total;
     }
 }
 
