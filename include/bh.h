@@ -457,9 +457,12 @@ const char* bh_renderer_last_error(bh_renderer* r);
  *   walk_stack_cap     stack entries a walk warp may use (0 = full; >= 2)
  *   flags              BH_DEBUG_LOOKBACK_UNPUBLISHED: the second tile of the
  *                      first sort pass waits on a predecessor status that
- *                      never reads as published (needs n > 6144 bodies)
+ *                      never reads as published (needs n > 6144 bodies);
+ *                      BH_DEBUG_SPLIT_BUILD: the split hierarchy build (local
+ *                      phase + frontier climb) at every body count
  * Zeros restore normal operation.  Takes effect from the next call. */
 #define BH_DEBUG_LOOKBACK_UNPUBLISHED 1u
+#define BH_DEBUG_SPLIT_BUILD 2u
 int bh_debug_set_limits(bh_sim* sim, uint32_t flags, uint32_t lookback_spin_cap,
                         uint32_t walk_stack_cap);
 

@@ -179,6 +179,54 @@ def test_split_build_matches_oracle_beyond_2m(bh, orc, cfg):
     sim.close()
 
 
+@pytest.mark.parametrize("n,scenario,cfg", [
+    (2, "default", dict(mortonDomain="bbox", softening="plummer")),
+    (3, "default", dict(walk="group", mortonDomain="bbox", softening="plummer")),
+    (511, "two-clusters", dict(walk="group", mortonDomain="bbox", softening="plummer")),
+    (5000, "default", dict(mortonDomain="bbox", softening="plummer")),
+    (70001, "gaussian-mixture", dict(walk="group", mortonBits=64, softening="plummer",
+                                     plummerEps=1e-4)),
+    (300000, "colliding-disks", dict(walk="group", mortonDomain="bbox", softening="plummer")),
+    (300000, "default", dict(mortonDomain="fixed2000")),   # the reference's duplicate-heavy keys
+], ids=["n2", "n3", "n511", "n5000-ref-layout", "n70001-64bit", "n300k", "n300k-fixed2000"])
+def test_split_build_every_size_matches_oracle(bh, orc, n, scenario, cfg):
+    """The split build (block-local phase, then the device-scope climb of
+    the frontier nodes it leaves) at sizes where the fused build normally
+    runs: tree arrays bit for bit against the oracle."""
+    sim = make_sim(bh, n, scenario, seed=2, **cfg)
+    sim.debugSetLimits(flags=bh.BH_DEBUG_SPLIT_BUILD)
+    bits64 = cfg.get("mortonBits") == 64
+    bbox = 1 if bits64 or cfg.get("mortonDomain") == "bbox" else 0
+    # reset, bbox, encode, sort passes, build (2 kernels), walk
+    assert sim.kernels_per_step() == 1 + bbox + 1 + (8 if bits64 else 4) + 2 + 1
+    compare_tree(orc, sim)
+    sim.close()
+
+
+@pytest.mark.parametrize("cfg", [
+    dict(walk="group", mortonDomain="bbox", softening="plummer", plummerEps=1e-3, deltaTime=1e-3),
+    dict(walk="group", mortonBits=64, softening="plummer", plummerEps=1e-4, deltaTime=1e-4,
+         integrator="leapfrog-kdk"),
+    dict(mortonDomain="bbox", softening="plummer", plummerEps=1e-3, deltaTime=1e-3),
+], ids=["group-32bit", "group-64bit-kdk", "exact-walk"])
+def test_split_build_steps_equal_fused_build(bh, cfg):
+    """Node records, and so every step, are bit-identical between the fused
+    build and the split build (same combine order, same FP64 rule): 200,000
+    bodies over 4 steps."""
+    n = 200000
+    runs = []
+    for flags in (0, bh.BH_DEBUG_SPLIT_BUILD):
+        sim = make_sim(bh, n, "colliding-disks", seed=9, **cfg)
+        sim.debugSetLimits(flags=flags)
+        sim.step(4)
+        m, p, v = sim.download()
+        t = sim.tree()
+        runs.append((p, v, t["node4"], t["aabb"], t["parent"]))
+        sim.close()
+    for x, y in zip(*runs):
+        assert np.array_equal(x, y)
+
+
 def test_headline_workload_tree_matches_oracle_800k(bh, orc):
     # The benchmark workload itself (800,000 bodies, two colliding disks,
     # 32-bit keys over the bounding box, group-walk records): every tree

@@ -5,8 +5,8 @@ The package directory name has hyphens, so load it with
 ``importlib.import_module("webgpu-fluid-sim_b200")`` after putting the
 repository root on ``sys.path``.
 """
-from ._lib import (BH_DEBUG_LOOKBACK_UNPUBLISHED, BH_ERR_DEVICE_CHECK, BH_OK,  # noqa: F401
-                   BhError, load)
+from ._lib import (BH_DEBUG_LOOKBACK_UNPUBLISHED, BH_DEBUG_SPLIT_BUILD,  # noqa: F401
+                   BH_ERR_DEVICE_CHECK, BH_OK, BhError, load)
 from .config import WORKLOADS, Config, getDefaultConfig  # noqa: F401
 from .render import RenderCommand, Renderer  # noqa: F401
 from .runlog import RunLog  # noqa: F401

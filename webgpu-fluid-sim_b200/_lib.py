@@ -30,6 +30,7 @@ BH_INTEGRATOR_LEAPFROG_KDK = 1
 BH_STAGE_NAMES = ("morton", "sort", "tree", "walk", "other")
 
 BH_DEBUG_LOOKBACK_UNPUBLISHED = 1
+BH_DEBUG_SPLIT_BUILD = 2
 
 
 class bh_config(ctypes.Structure):

@@ -45,6 +45,8 @@ constexpr uint32_t kSpinCapDefault = 1u << 22;
 // Test hook: the second tile of the first sort pass waits on a predecessor
 // status that never reads as published, so its bounded wait runs out.
 constexpr uint32_t kDebugLookbackUnpublished = 1u << 0;
+// the split hierarchy build (local phase + frontier climb) at every body count from 2
+constexpr uint32_t kDebugSplitBuild = 1u << 1;
 
 // Packed internal-node record of the group walk (64 B, one per internal node):
 // the criterion reads `box`, an accepted node contributes `mom` + `quad`, an
@@ -230,7 +232,7 @@ void launch_build_fill(const DeviceBuffers& b, int fp64_levels, cudaStream_t s);
 #define BH_SPLIT_BUILD_MIN (1u << 21)
 #endif
 constexpr uint32_t kSplitBuildMin = BH_SPLIT_BUILD_MIN;
-bool split_build(uint32_t n);
+bool split_build(uint32_t n, uint32_t debug_flags);
 void launch_ref_layout(const DeviceBuffers& b, cudaStream_t s);  // group walk: node4/aabb/children/range on request
 void init_bound(const DeviceBuffers& b, cudaStream_t s);
 // walk.cu

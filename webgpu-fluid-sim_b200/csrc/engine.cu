@@ -1327,7 +1327,7 @@ extern "C" int bh_walk_stats(bh_sim* s, uint64_t* node_visits, uint64_t* multipo
 extern "C" int bh_debug_set_limits(bh_sim* s, uint32_t flags, uint32_t lookback_spin_cap,
                                    uint32_t walk_stack_cap) {
     BH_HANDLE(s);
-    if (flags & ~bh::kDebugLookbackUnpublished)
+    if (flags & ~(bh::kDebugLookbackUnpublished | bh::kDebugSplitBuild))
         return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_debug_set_limits: unknown flag");
     if (walk_stack_cap == 1)
         return fail(s, BH_ERR_INVALID_ARGUMENT, "bh_debug_set_limits: a walk stack needs 2 entries");
@@ -1543,7 +1543,7 @@ extern "C" int bh_kernels_per_step(bh_sim* s, uint32_t* out) {
     if (needs_bbox(s) || s->b.num_systems) k += 1;                 // bbox (per system)
     k += 1;                                                         // encode
     k += (uint32_t)bh::sort_passes(s->b);                          // sort passes
-    k += bh::split_build(s->b.n) ? 2 : 1;                           // build + fill (+ frontier climb)
+    k += bh::split_build(s->b.n, s->b.debug_flags) ? 2 : 1;                           // build + fill (+ frontier climb)
     k += 1;                                                         // walk + integrate
     *out = s->b.n ? k : 0;
     return BH_OK;

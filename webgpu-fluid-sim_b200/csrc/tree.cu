@@ -6,7 +6,9 @@
 
 namespace bh {
 
-bool split_build(uint32_t n) { return n >= kSplitBuildMin; }
+bool split_build(uint32_t n, uint32_t debug_flags) {
+    return n >= kSplitBuildMin || (n >= 2 && (debug_flags & kDebugSplitBuild));
+}
 
 template <typename K, bool SPLIT>
 static cudaError_t set_build_attributes() {
@@ -51,7 +53,7 @@ static void launch_typed(const DeviceBuffers& b, int fp64_levels, cudaStream_t s
     a.gmax = b.group_max;
     a.xm = b.xm;
     a.err = b.err;
-    if (!split_build(b.n)) {
+    if (!split_build(b.n, b.debug_flags)) {
         constexpr uint32_t B = build_block<false>();
         build_fill_kernel<K, false><<<(b.n + B - 1) / B, B, sizeof(BuildShared<K, B>), s>>>(a);
         return;
