@@ -56,8 +56,12 @@ PKG = "webgpu-fluid-sim_b200"
 DEFAULT_WORKLOAD = "colliding-disks-800k"
 FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes (read + write) of one launch of the dominant kernel (the walk),
-# from one ncu capture of the same workload.
-NCU_WALK_TRAFFIC_BYTES = {"colliding-disks-800k": 72.04e6}  # far-field walk, 128-body groups
+# from one ncu capture of the same workload; the 16.8M point from a capture
+# of its 4.2M-body case (same generator and settings, 1.364 GB) scaled by
+# the bodies processed.
+NCU_WALK_TRAFFIC_BYTES = {"colliding-disks-800k": 72.04e6,  # far-field walk, 128-body groups
+                          "gaussian-mixture-4m": 1.364e9,
+                          "gaussian-mixture-16m": 1.364e9 * 4.0}
 # Algorithmic HBM bytes per body and step of the stream stages: encode =
 # position 8 + mass 4 read, key 4|8 + packed leaf record 16 written; sort =
 # first pass key read + key and id written, later passes key and id read and
@@ -287,8 +291,10 @@ def secondary_16m(pkg, device: int, steps: int = 5, e2e_steps: int = 3, sm_max_m
     out = {"workload": "gaussian-mixture-16m", "bodies": n, "metric": "body-steps/s",
            "value": n / (ms / 1e3), "unit": "body-steps/s", "ms_per_step": ms, "steps": steps,
            "stages_ms": stages,
-           "roofline": walk_roofline(cfg, stages["walk"], multi, body, visits, sm_max_mhz,
-                                     far_pairs=far, n=n),
+           "roofline": dict(walk_roofline(cfg, stages["walk"], multi, body, visits, sm_max_mhz,
+                                          traffic=NCU_WALK_TRAFFIC_BYTES["gaussian-mixture-16m"],
+                                          far_pairs=far, n=n),
+                            traffic_source="ncu capture of the 4.2M-body case scaled by 4"),
            "stream_stages": stream_rooflines(stages, n, 8, hbm_gbs),
            "force_error_vs_fp64": ferr, "e2e": e2e, "autotune": tune,
            "gpu_launches": kps * steps,

@@ -261,6 +261,40 @@ def test_headline_workload_tree_matches_oracle_800k(bh, orc):
     sim.close()
 
 
+def test_metric_workload_tree_matches_oracle_16m(bh, orc):
+    # The 16.8M-body point of the metric (Gaussian mixture with 1% exact
+    # duplicates, 64-bit keys, split build): every tree array bit for bit
+    # against the oracle, node values within tolerance, and the force error
+    # against the FP64 direct sum on 1,024 bodies.
+    wl = bh.WORKLOADS["gaussian-mixture-16m"]
+    n = wl["n"]
+    sim = bh.Simulation(wl["config"])
+    sim.setNumBodies(n)
+    sim.setScenario(wl["scenario"], 1)
+    mass, pos, vel = sim.download()
+    acc = sim.computeAccelerations()
+    t = sim.tree()
+    p = orc.params_from_config(sim.config)
+    codes, ids = orc.morton(p, pos)
+    codes, ids = orc.sort(codes, ids)
+    assert (t["codes"] == codes).all(), "Morton codes differ"
+    assert (t["ids"] == ids).all(), "sorted permutation differs"
+    left, right, parent = orc.build(codes, sim.config.mortonBits)
+    assert (t["parent"] == parent).all(), "parent array differs"
+    assert (t["children"][:, 0] == left[: n - 1]).all(), "left children differ"
+    assert (t["children"][:, 1] == right[: n - 1]).all(), "right children differ"
+    com, mnode, aabb, length = orc.fill(ids, mass, pos, left, right, parent)
+    assert (t["aabb"] == aabb[: n - 1]).all(), "AABBs differ"
+    assert (t["node4"][:, 3] == length).all(), "lengths differ"
+    assert np.all(np.abs(t["node4"][:, 2] - mnode) <= 1e-5 * np.abs(mnode) + 1e-30)
+    scale = np.abs(com).max(1) + length
+    assert np.all(np.abs(t["node4"][:, :2] - com).max(1) <= 1e-5 * scale + 1e-30)
+    fe = sim.forceError(acc, nsample=1024, seed=5)
+    print(f"16.8M group walk: FP64 error median {fe['median']:.3e} p99 {fe['p99']:.3e}")
+    assert fe["median"] <= 1e-3
+    sim.close()
+
+
 def test_direct_forces_fp64_matches_oracle(bh, orc):
     # The GPU FP64 direct sum used to measure every force error, against the
     # oracle's FP64 direct sum (both softening laws).
