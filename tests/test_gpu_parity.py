@@ -52,6 +52,23 @@ def compare_tree(orc, sim, check_values=True):
     return acc, acc_ref
 
 
+def node_body_counts(left, right, n):
+    """Bodies under every node of the Karras numbering (internal nodes
+    [0, n-2], leaves n-1+slot), from the child arrays, level by level."""
+    nm1 = n - 1
+    L, R = left.astype(np.int64), right.astype(np.int64)
+    cnt = np.ones(2 * n - 1, np.int64)
+    levels, fr = [], np.array([0])
+    while fr.size:
+        levels.append(fr)
+        inner = fr[fr < nm1]
+        fr = np.concatenate([L[inner], R[inner]])
+    for lv in reversed(levels):
+        inner = lv[lv < nm1]
+        cnt[inner] = cnt[L[inner]] + cnt[R[inner]]
+    return cnt
+
+
 def acc_errors(acc, acc_ref):
     num = np.linalg.norm(acc.astype(np.float64) - acc_ref, axis=1)
     den = np.linalg.norm(acc_ref.astype(np.float64), axis=1)
@@ -255,6 +272,12 @@ def test_headline_workload_tree_matches_oracle_800k(bh, orc):
     assert np.all(np.abs(t["node4"][:, 2] - mnode) <= 1e-5 * np.abs(mnode) + 1e-30)
     scale = np.abs(com).max(1) + length
     assert np.all(np.abs(t["node4"][:, :2] - com).max(1) <= 1e-5 * scale + 1e-30)
+    # Nodes below the FP64 threshold take the reference's f32 formula
+    # (lbvh.wgsl:216-224) with every operation rounded as the oracle rounds
+    # it, the division included: bit for bit, on every such node.
+    small = node_body_counts(left, right, n) < 1024
+    assert (t["node4"][small, 2] == mnode[small]).all(), "f32 node masses differ"
+    assert (t["node4"][small, :2] == com[small]).all(), "f32 node centres differ"
     fe = sim.forceError(acc, nsample=2048, seed=5)
     print(f"800k group walk: FP64 error median {fe['median']:.3e} p99 {fe['p99']:.3e}")
     assert fe["median"] <= 1e-3

@@ -54,6 +54,19 @@
 
 namespace bh {
 
+// a / b correctly rounded, given r = 1/b correctly rounded (__frcp_rn): one
+// correction of the product a r by its exact residual a - b (a r) (an FMA),
+// P. Markstein's final step for IEEE division (IBM J. Res. Dev. 34(1), 1990):
+// with r within half an ulp of 1/b and q within an ulp of a/b, q + (a - b q) r
+// rounds to a/b.  Operands here are normal-range masses and mass moments
+// (b > 0); the build divides two numerators by one mass, so the reciprocal
+// is shared and each quotient costs a multiply and two FMAs.
+__device__ __forceinline__ float div_by(float a, float b, float r) {
+    const float q = __fmul_rn(a, r);
+    const float e = __fmaf_rn(-q, b, a);
+    return __fmaf_rn(e, r, q);
+}
+
 template <typename K>
 __device__ __forceinline__ int delta_at(const K* __restrict__ keys, uint32_t i, uint32_t j) {
     K a = __ldg(&keys[i]), b = __ldg(&keys[j]);
@@ -275,8 +288,9 @@ __device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, Buil
             c.dmx += smx;
             c.dmy += smy;
             tm = (float)c.dm;
-            ncx = c.dm > 0.0 ? (float)(c.dmx / c.dm) : 0.0f;
-            ncy = c.dm > 0.0 ? (float)(c.dmy / c.dm) : 0.0f;
+            const double inv = c.dm > 0.0 ? 1.0 / c.dm : 0.0;
+            ncx = (float)(c.dmx * inv);
+            ncy = (float)(c.dmy * inv);
             A.big[2 * (size_t)pidx] = make_double2(c.dm, c.dmx);
             A.big[2 * (size_t)pidx + 1] = make_double2(c.dmy, 0.0);
         } else {
@@ -285,8 +299,9 @@ __device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, Buil
             else { ml = s4.z; clx = s4.x; cly = s4.y; mr = c.cm; crx = c.cx; cry = c.cy; }
             tm = __fadd_rn(ml, mr);
             if (tm > 0.0f) {
-                ncx = __fdiv_rn(__fadd_rn(__fmul_rn(clx, ml), __fmul_rn(crx, mr)), tm);
-                ncy = __fdiv_rn(__fadd_rn(__fmul_rn(cly, ml), __fmul_rn(cry, mr)), tm);
+                const float inv = __frcp_rn(tm);
+                ncx = div_by(__fadd_rn(__fmul_rn(clx, ml), __fmul_rn(crx, mr)), tm, inv);
+                ncy = div_by(__fadd_rn(__fmul_rn(cly, ml), __fmul_rn(cry, mr)), tm, inv);
             } else {
                 ncx = 0.0f;
                 ncy = 0.0f;
@@ -304,12 +319,11 @@ __device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, Buil
                 ml = s4.z; lxx = sq.x; lxy = sq.y; lyy = sq.z; dlx = __fsub_rn(s4.x, ncx); dly = __fsub_rn(s4.y, ncy);
                 mr = c.cm; rxx = c.sxx; rxy = c.sxy; ryy = c.syy; drx = __fsub_rn(c.cx, ncx); dry = __fsub_rn(c.cy, ncy);
             }
-            c.sxx = __fadd_rn(__fadd_rn(lxx, __fmul_rn(ml, __fmul_rn(dlx, dlx))),
-                              __fadd_rn(rxx, __fmul_rn(mr, __fmul_rn(drx, drx))));
-            c.sxy = __fadd_rn(__fadd_rn(lxy, __fmul_rn(ml, __fmul_rn(dlx, dly))),
-                              __fadd_rn(rxy, __fmul_rn(mr, __fmul_rn(drx, dry))));
-            c.syy = __fadd_rn(__fadd_rn(lyy, __fmul_rn(ml, __fmul_rn(dly, dly))),
-                              __fadd_rn(ryy, __fmul_rn(mr, __fmul_rn(dry, dry))));
+            const float mdlx = __fmul_rn(ml, dlx), mdly = __fmul_rn(ml, dly);
+            const float mdrx = __fmul_rn(mr, drx), mdry = __fmul_rn(mr, dry);
+            c.sxx = __fadd_rn(__fmaf_rn(mdlx, dlx, lxx), __fmaf_rn(mdrx, drx, rxx));
+            c.sxy = __fadd_rn(__fmaf_rn(mdlx, dly, lxy), __fmaf_rn(mdrx, dry, rxy));
+            c.syy = __fadd_rn(__fmaf_rn(mdly, dly, lyy), __fmaf_rn(mdry, dry, ryy));
             GNode g;
             g.box = make_float4(c.lox, c.loy, c.hix, c.hiy);
             g.mom = make_float4(ncx, ncy, tm, len);
