@@ -294,9 +294,16 @@ __device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, Buil
             A.big[2 * (size_t)pidx] = make_double2(c.dm, c.dmx);
             A.big[2 * (size_t)pidx + 1] = make_double2(c.dmy, 0.0);
         } else {
-            float ml, mr, clx, cly, crx, cry;
-            if (is_left) { ml = c.cm; clx = c.cx; cly = c.cy; mr = s4.z; crx = s4.x; cry = s4.y; }
-            else { ml = s4.z; clx = s4.x; cly = s4.y; mr = c.cm; crx = c.cx; cry = c.cy; }
+            // (c_l m_l + c_r m_r) / (m_l + m_r).  Each sum is one IEEE addition
+            // of two terms, which is commutative, so this node's and the
+            // sibling's terms may be summed in either order with the same
+            // result; the split build's kernels (B >= 256) skip the left/right
+            // selects (16.8M-case build 5% faster), the fused build keeps
+            // them (measured 2.5% faster at 800k with them).
+            float ml = c.cm, mr = s4.z, clx = c.cx, cly = c.cy, crx = s4.x, cry = s4.y;
+            if (B < 256 && !is_left) {
+                ml = s4.z; clx = s4.x; cly = s4.y; mr = c.cm; crx = c.cx; cry = c.cy;
+            }
             tm = __fadd_rn(ml, mr);
             if (tm > 0.0f) {
                 const float inv = __frcp_rn(tm);
@@ -309,21 +316,24 @@ __device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, Buil
         }
         const float len = fmaxf(__fsub_rn(c.hix, c.lox), __fsub_rn(c.hiy, c.loy));
         if (A.gnode) {
-            // Second moments about the parent COM, left child first:
-            // S = sum_c S_c + m_c d_c d_c^T, d_c = c_c - c_parent (leaves: S_c = 0).
-            float ml, mr, lxx, lxy, lyy, rxx, rxy, ryy, dlx, dly, drx, dry;
-            if (is_left) {
-                ml = c.cm; lxx = c.sxx; lxy = c.sxy; lyy = c.syy; dlx = __fsub_rn(c.cx, ncx); dly = __fsub_rn(c.cy, ncy);
-                mr = s4.z; rxx = sq.x; rxy = sq.y; ryy = sq.z; drx = __fsub_rn(s4.x, ncx); dry = __fsub_rn(s4.y, ncy);
-            } else {
-                ml = s4.z; lxx = sq.x; lxy = sq.y; lyy = sq.z; dlx = __fsub_rn(s4.x, ncx); dly = __fsub_rn(s4.y, ncy);
-                mr = c.cm; rxx = c.sxx; rxy = c.sxy; ryy = c.syy; drx = __fsub_rn(c.cx, ncx); dry = __fsub_rn(c.cy, ncy);
+            // Second moments about the parent COM:
+            // S = sum_c S_c + m_c d_c d_c^T, d_c = c_c - c_parent (leaves: S_c = 0),
+            // the two children's terms joined by one (commutative) addition;
+            // a and b are this node and its sibling, or (fused build) the
+            // left and the right child, as for the centre above.
+            float ma = c.cm, mb = s4.z, sax = c.sxx, say = c.sxy, saz = c.syy;
+            float sbx = sq.x, sby = sq.y, sbz = sq.z, pax = c.cx, pay = c.cy, pbx = s4.x, pby = s4.y;
+            if (B < 256 && !is_left) {
+                ma = s4.z; sax = sq.x; say = sq.y; saz = sq.z; pax = s4.x; pay = s4.y;
+                mb = c.cm; sbx = c.sxx; sby = c.sxy; sbz = c.syy; pbx = c.cx; pby = c.cy;
             }
-            const float mdlx = __fmul_rn(ml, dlx), mdly = __fmul_rn(ml, dly);
-            const float mdrx = __fmul_rn(mr, drx), mdry = __fmul_rn(mr, dry);
-            c.sxx = __fadd_rn(__fmaf_rn(mdlx, dlx, lxx), __fmaf_rn(mdrx, drx, rxx));
-            c.sxy = __fadd_rn(__fmaf_rn(mdlx, dly, lxy), __fmaf_rn(mdrx, dry, rxy));
-            c.syy = __fadd_rn(__fmaf_rn(mdly, dly, lyy), __fmaf_rn(mdry, dry, ryy));
+            const float dax = __fsub_rn(pax, ncx), day = __fsub_rn(pay, ncy);
+            const float dbx = __fsub_rn(pbx, ncx), dby = __fsub_rn(pby, ncy);
+            const float madx = __fmul_rn(ma, dax), mady = __fmul_rn(ma, day);
+            const float mbdx = __fmul_rn(mb, dbx), mbdy = __fmul_rn(mb, dby);
+            c.sxx = __fadd_rn(__fmaf_rn(madx, dax, sax), __fmaf_rn(mbdx, dbx, sbx));
+            c.sxy = __fadd_rn(__fmaf_rn(madx, day, say), __fmaf_rn(mbdx, dby, sby));
+            c.syy = __fadd_rn(__fmaf_rn(mady, day, saz), __fmaf_rn(mbdy, dby, sbz));
             GNode g;
             g.box = make_float4(c.lox, c.loy, c.hix, c.hiy);
             g.mom = make_float4(ncx, ncy, tm, len);
