@@ -158,9 +158,73 @@ struct BuildShared {
     int suf[B];             // suf[q] = min of d[q+1..B]
     unsigned char local[B + 1];
     uint32_t bound[B + 1];  // exchange slots of the local splits
-    float leaf[3][B];       // leaf {m, x, y} by slot - B0
-    float rec[10][B];       // local internal node {m, cx, cy, box, S} by index - B0
+    // Leaves by slot - B0 and local internal nodes by index - B0: float4
+    // records ({x, y, m, 0}; {cx, cy, m, 0}, box, {S, 0}) for the split
+    // build's large CTAs, separate float arrays ([3][B] {m, x, y}; [10][B]
+    // {m, cx, cy, box, S}) for the fused build's small ones -- each measured
+    // the faster layout for its kernel.
+    static constexpr bool kVec = B >= 256;
+    alignas(16) float leaf[kVec ? 4 * B : 3 * B];
+    alignas(16) float rec[kVec ? 12 * B : 10 * B];
 };
+
+// Record access in either layout of BuildShared.  Reads follow the block
+// fence after the exchange and writes precede the next one, which orders
+// them (the fence is also a compiler barrier); the separate arrays are read
+// and written through volatile pointers as before.
+template <typename K, int B>
+__device__ __forceinline__ float4 shared_leaf(BuildShared<K, B>* S, int k) {
+    if constexpr (BuildShared<K, B>::kVec) return reinterpret_cast<const float4*>(S->leaf)[k];
+    const volatile float* v = S->leaf;
+    return make_float4(v[B + k], v[2 * B + k], v[k], 0.f);
+}
+template <typename K, int B>
+__device__ __forceinline__ void put_leaf(BuildShared<K, B>* S, int k, float4 r) {
+    if constexpr (BuildShared<K, B>::kVec) {
+        reinterpret_cast<float4*>(S->leaf)[k] = r;
+    } else {
+        S->leaf[k] = r.z;
+        S->leaf[B + k] = r.x;
+        S->leaf[2 * B + k] = r.y;
+    }
+}
+template <typename K, int B>
+__device__ __forceinline__ void shared_rec(BuildShared<K, B>* S, int k, float4& mom, float4& box,
+                                           float4& quad) {
+    if constexpr (BuildShared<K, B>::kVec) {
+        const float4* r = reinterpret_cast<const float4*>(S->rec);
+        mom = r[k];
+        box = r[B + k];
+        quad = r[2 * B + k];
+    } else {
+        const volatile float* v = S->rec;
+        mom = make_float4(v[B + k], v[2 * B + k], v[k], 0.f);
+        box = make_float4(v[3 * B + k], v[4 * B + k], v[5 * B + k], v[6 * B + k]);
+        quad = make_float4(v[7 * B + k], v[8 * B + k], v[9 * B + k], 0.f);
+    }
+}
+template <typename K, int B>
+__device__ __forceinline__ void put_rec(BuildShared<K, B>* S, int k, float4 mom, float4 box,
+                                        float4 quad) {
+    if constexpr (BuildShared<K, B>::kVec) {
+        float4* r = reinterpret_cast<float4*>(S->rec);
+        r[k] = mom;
+        r[B + k] = box;
+        r[2 * B + k] = quad;
+    } else {
+        volatile float* v = S->rec;
+        v[k] = mom.z;
+        v[B + k] = mom.x;
+        v[2 * B + k] = mom.y;
+        v[3 * B + k] = box.x;
+        v[4 * B + k] = box.y;
+        v[5 * B + k] = box.z;
+        v[6 * B + k] = box.w;
+        v[7 * B + k] = quad.x;
+        v[8 * B + k] = quad.y;
+        v[9 * B + k] = quad.z;
+    }
+}
 
 // The node a climbing thread currently owns: its slot range, the deltas at
 // the range's two boundaries, and its record.
@@ -187,8 +251,6 @@ __device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, Buil
                                            uint32_t B0) {
     const uint32_t n = A.n, nm1 = n - 1;
     bool local = LOCAL && c.local;
-    volatile float* vrec = LOCAL ? &S->rec[0][0] : nullptr;
-    volatile float* vleaf = LOCAL ? &S->leaf[0][0] : nullptr;
     {
         const bool is_left = c.dr > c.dl;
         const uint32_t gamma = is_left ? c.r : c.l - 1;
@@ -234,13 +296,11 @@ __device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, Buil
             // Sibling record from shared memory.
             if (sib >= nm1) {
                 const int k = (int)(sib - nm1 - B0);
-                s4 = make_float4(vleaf[B + k], vleaf[2 * B + k], vleaf[k], 0.f);
+                s4 = shared_leaf(S, k);
                 sb = make_float4(s4.x, s4.y, s4.x, s4.y);
             } else {
                 const int k = (int)(sib - B0);
-                s4 = make_float4(vrec[B + k], vrec[2 * B + k], vrec[k], 0.f);
-                sb = make_float4(vrec[3 * B + k], vrec[4 * B + k], vrec[5 * B + k], vrec[6 * B + k]);
-                sq = make_float4(vrec[7 * B + k], vrec[8 * B + k], vrec[9 * B + k], 0.f);
+                shared_rec(S, k, s4, sb, sq);
             }
         } else if (sib >= nm1) {
             // Sibling record through L2 (written by another thread in this launch).
@@ -371,16 +431,8 @@ __device__ __forceinline__ bool climb_step(const BuildArgs<K>& A, Climb& c, Buil
         if (IN_LOCAL) {
             // the new node is local: its record for the sibling that may meet it here
             const int k = (int)(pidx - B0);
-            vrec[k] = tm;
-            vrec[B + k] = ncx;
-            vrec[2 * B + k] = ncy;
-            vrec[3 * B + k] = c.lox;
-            vrec[4 * B + k] = c.loy;
-            vrec[5 * B + k] = c.hix;
-            vrec[6 * B + k] = c.hiy;
-            vrec[7 * B + k] = c.sxx;
-            vrec[8 * B + k] = c.sxy;
-            vrec[9 * B + k] = c.syy;
+            put_rec(S, k, make_float4(ncx, ncy, tm, 0.0f), make_float4(c.lox, c.loy, c.hix, c.hiy),
+                    make_float4(c.sxx, c.sxy, c.syy, 0.0f));
         }
         c.cm = tm; c.cx = ncx; c.cy = ncy;
         c.l = pl;
@@ -498,9 +550,7 @@ build_fill_kernel(const BuildArgs<K> A) {
         p = __ldg(&A.pos[body]);
     }
     A.node4[nm1 + i] = make_float4(p.x, p.y, m, 0.0f);  // leaf (lbvh.wgsl:179-187)
-    S.leaf[0][t] = m;
-    S.leaf[1][t] = p.x;
-    S.leaf[2][t] = p.y;
+    put_leaf(&S, t, make_float4(p.x, p.y, m, 0.0f));
     Climb c;
     c.l = i;
     c.r = i;
