@@ -103,6 +103,30 @@ def test_rollout_gradient_matches_fp64_adjoint_4096(bh, orc):
 
 
 @pytest.mark.gpu
+def test_rollout_gradient_split_build_equals_fused_build(bh):
+    """The rollout gradient rebuilds a tree per replayed step; with the split
+    build forced (what runs from 2^21 bodies) the trees, the rollout and its
+    loss are the fused build's bit for bit, and the gradients agree to the
+    rounding of their float atomic sums (the VJP scatters node adjoints with
+    atomics, whose order varies from run to run)."""
+    n, steps = 4096, 40
+    mass, pos, vel, tgt = _target(bh, n, 8, steps)
+    out = []
+    for flags in (0, bh.BH_DEBUG_SPLIT_BUILD):
+        sim = bh.Simulation(adjoint_config(bh))
+        sim.setNumBodies(n)
+        sim.debugSetLimits(flags=flags)
+        sim.upload(mass, pos, vel)
+        out.append(sim.rollout_grad(steps, 20, tgt))
+        sim.close()
+    (L0, *g0), (L1, *g1) = out
+    assert L0 == L1
+    for a, b in zip(g0, g1):
+        rel = float(np.linalg.norm(a.astype(np.float64) - b) / np.linalg.norm(b.astype(np.float64)))
+        assert rel <= 1e-5, rel
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("n,steps,leaf", [(4096, 200, 8), (65536, 200, 4)])
 def test_rollout_gradient_matches_finite_differences(bh, n, steps, leaf):
     """Central differences of the engine's own FP32 loss along one random

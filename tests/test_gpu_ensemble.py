@@ -124,3 +124,23 @@ def test_ensemble_1024_systems_accuracy_vs_fp64(bh, orc):
     assert np.median(np.concatenate(errs)) <= 1e-3
     assert ens.kernels_per_step() >= 5
     ens.close()
+
+
+def test_ensemble_split_build_equals_fused_build(bh):
+    """Large ensembles (the benchmark's 4.9e7 bodies) build their tree with
+    the split build; forced on a small ensemble it gives the same tree and
+    the same steps as the fused build, bit for bit."""
+    sizes = [3000, 700, 5000, 12000]
+    cfg = bh.Config(**dict(GROUP, integrator="symplectic-euler", deltaTime=1e-4))
+    runs = []
+    for flags in (0, bh.BH_DEBUG_SPLIT_BUILD):
+        ens = bh.Ensemble(sizes, cfg)
+        ens.setScenarios(None, seed=6)
+        ens.debugSetLimits(flags=flags)
+        ens.step(3)
+        _, p, v = ens.download()
+        t = ens.tree()
+        runs.append((p, v, t["node4"], t["parent"]))
+        ens.close()
+    for x, y in zip(*runs):
+        assert np.array_equal(x, y)
