@@ -116,13 +116,14 @@ int bh_update_metadata(bh_sim* sim);
  * to skip that array.  bh_upload is asynchronous for page-locked host
  * memory, which must stay valid until the copies are done (the next
  * bh_sync or bh_download).  The copies run on a second copy stream of the
- * handle: positions into a device staging buffer at once (they may overlap
- * steps still running; the handle's stream moves them into place before
- * their next reader), then masses and velocities, ordered after everything
- * enqueued before.  The next step's stages before their first reader (the
- * hierarchy build for the masses, the walk for the velocities) do not wait
- * for them; every other call orders the handle's stream after them.
- * bh_download synchronises before returning. */
+ * handle, positions first, then masses, then velocities, each into its own
+ * device staging buffer as soon as the previous upload of that array has
+ * been moved out of it, so they may overlap steps still running; the
+ * handle's stream moves each array into place before its next reader.  The
+ * next step's stages before those readers (the hierarchy build for the
+ * masses, the walk for the velocities) do not wait for them; every other
+ * call orders the handle's stream after them.  bh_download synchronises
+ * before returning. */
 int bh_upload(bh_sim* sim, const float* mass, const float* pos, const float* vel, uint32_t n);
 int bh_download(bh_sim* sim, float* mass, float* pos, float* vel, uint32_t n);
 
