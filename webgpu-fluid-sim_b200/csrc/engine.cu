@@ -106,21 +106,26 @@ static thread_local std::string g_err;
 // stream.  Every entry point calls settle_uploads (through BH_HANDLE) before
 // it touches the body buffers, except bh_upload and bh_step, which order the
 // copies themselves.
-static void settle(const bh_sim* s, int k, void* dst) {
+// Returns the first CUDA error; the array stays pending unless all three
+// calls were enqueued.
+static cudaError_t settle(const bh_sim* s, int k, void* dst) {
     const bh_sim::Staged& u = s->up[k];
-    if (!u.pending) return;
-    cudaStreamWaitEvent(s->stream, u.landed, 0);
-    cudaMemcpyAsync(dst, u.buf, u.width * (size_t)s->b.n, cudaMemcpyDeviceToDevice, s->stream);
-    cudaEventRecord(u.freed, s->stream);
-    u.pending = false;
+    if (!u.pending) return cudaSuccess;
+    cudaError_t e = cudaStreamWaitEvent(s->stream, u.landed, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dst, u.buf, u.width * (size_t)s->b.n, cudaMemcpyDeviceToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(u.freed, s->stream);
+    if (e == cudaSuccess) u.pending = false;
+    return e;
 }
-static void settle_pos(const bh_sim* s) { settle(s, bh_sim::kPos, s->b.pos); }
-static void settle_mass(const bh_sim* s) { settle(s, bh_sim::kMass, s->b.mass); }
-static void settle_vel(const bh_sim* s) { settle(s, bh_sim::kVel, s->b.vel); }
-static void settle_uploads(const bh_sim* s) {
-    settle_pos(s);
-    settle_mass(s);
-    settle_vel(s);
+static cudaError_t settle_pos(const bh_sim* s) { return settle(s, bh_sim::kPos, s->b.pos); }
+static cudaError_t settle_mass(const bh_sim* s) { return settle(s, bh_sim::kMass, s->b.mass); }
+static cudaError_t settle_vel(const bh_sim* s) { return settle(s, bh_sim::kVel, s->b.vel); }
+static cudaError_t settle_uploads(const bh_sim* s) {
+    cudaError_t e = settle_pos(s);
+    if (e == cudaSuccess) e = settle_mass(s);
+    if (e == cudaSuccess) e = settle_vel(s);
+    return e;
 }
 
 namespace bh {
@@ -134,7 +139,10 @@ namespace bh {
 bool sim_body_view(const bh_sim* s, BodyView* out) {
     if (!s || !out) return false;
     cudaSetDevice(s->device);  // settling may copy staged positions on the handle's stream
-    settle_uploads(s);  // callers use the buffers on the handle's stream
+    // Callers use the buffers on the handle's stream.  A settling error (a
+    // broken context) also fails their own launches, which report it; the
+    // view is filled either way so no caller sees null buffers.
+    settle_uploads(s);
     out->mass = s->b.mass;
     out->pos = s->b.pos;
     out->vel = s->b.vel;
@@ -616,7 +624,8 @@ static int check_device_errors(bh_sim* s) {
 #define BH_HANDLE(s)                                                                        \
     do {                                                                                    \
         BH_HANDLE_NO_SETTLE(s);                                                             \
-        settle_uploads(s);                                                                  \
+        cudaError_t _u = settle_uploads(s);                                                 \
+        if (_u != cudaSuccess) return cuda_fail((s), _u, "settling staged uploads");        \
     } while (0)
 
 // ---- lifetime ------------------------------------------------------------------
@@ -965,10 +974,10 @@ extern "C" int bh_download_async(bh_sim* s, float* mass, float* pos, float* vel,
 static int step_once(bh_sim* s) {
     const bool kdk = s->cfg.integrator == BH_INTEGRATOR_LEAPFROG_KDK;
     cudaEvent_t* ev = prof_slot(s);
-    settle_pos(s);  // the reset and bounding box come first: positions are read at once
+    BH_CUDA(s, settle_pos(s));  // the reset and bounding box come first: positions are read at once
     const bool overlap = (s->up[bh_sim::kMass].pending || s->up[bh_sim::kVel].pending) && !kdk && !ev &&
                          s->cfg.use_graphs;
-    if (!overlap) settle_uploads(s);  // leapfrog reads both at once (force evaluation, opening kick)
+    if (!overlap) BH_CUDA(s, settle_uploads(s));  // leapfrog reads both at once (force evaluation, opening kick)
     if (kdk && !s->acc_valid) {
         enqueue_forces(s, [](int) {});  // first force evaluation of a leapfrog run
         s->acc_valid = true;
@@ -990,12 +999,12 @@ static int step_once(bh_sim* s) {
             }
         if (m) {
             BH_CUDA(s, cudaGraphLaunch(s->exec[4], s->stream));
-            settle_mass(s);
+            BH_CUDA(s, settle_mass(s));
             BH_CUDA(s, cudaGraphLaunch(s->exec[5], s->stream));
         } else {
             BH_CUDA(s, cudaGraphLaunch(s->exec[2], s->stream));
         }
-        settle_vel(s);
+        BH_CUDA(s, settle_vel(s));
         BH_CUDA(s, cudaGraphLaunch(s->exec[3], s->stream));
         s->acc_valid = false;
         return BH_OK;
