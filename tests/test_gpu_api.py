@@ -181,9 +181,9 @@ def test_velocity_upload_overlap_on_an_ensemble(bh):
 
 @pytest.mark.parametrize("n", [1, 2, 300, 12000])
 def test_partial_uploads_overlapping_the_step(bh, n):
-    """Uploads of some arrays only (all travel on the copy stream, the
-    positions through the staging buffer), each followed by a step:
-    bit-equal to waiting for the upload, down to one and two bodies."""
+    """Uploads of some arrays only (each travels on the copy stream into its
+    own staging buffer), each followed by a step: bit-equal to waiting for
+    the upload, down to one and two bodies."""
     cfg = dict(walk="group", softening="plummer", plummerEps=1e-3, mortonDomain="bbox",
                integrator="symplectic-euler", deltaTime=1e-3)
     a = _sim(bh, n=n, **cfg)
