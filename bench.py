@@ -26,8 +26,15 @@ Reference arm (--impl reference): the reference's own pipeline logic on the
 host cores: its WGSL compute shaders mechanically translated to C++
 (oracle/_ref, built where the reference checkout exists), all host threads;
 if that build is absent, the oracle port.  The WGSL itself needs a WebGPU
-device, which this machine lacks.  That arm imports nothing from the engine
-package: its inputs come from the oracle's generators.
+device, which this machine lacks.  W untimed steps, then exactly K timed
+steps, each a bounded sample of the workload (the walk on every k-th sorted
+slot, scaled by k, when a whole step would not fit the run's few minutes).
+That arm imports nothing from the engine package: its inputs come from the
+oracle's generators.
+
+Both arms print the same `config` (the workload, the parallelism and the
+cache treatment); the own arm's implementation choices (key width, walk
+shape, autotuning) are in its `engine` object.
 
 Multi-GPU (torchrun): by default one system on all ranks (--shard: every
 rank builds the same tree, walks its range of sorted slots, and the ranks
@@ -601,41 +608,111 @@ def _oracle():
     return orc
 
 
-def reference_baseline(wp: dict, seconds_budget=20.0):
-    """The reference's own shader logic (oracle/_ref: a mechanical C++
-    translation of lbvh.wgsl + barnes_hut.wgsl, independent stages on all host
-    threads) on the workload's bodies, theta and dt.  The bodies come from the
-    oracle's generator (one PCG32 stream per body: the workload's distribution
-    and size).  The reference knows only its own softening, eps = epsMult
+def _ref_setup(wp: dict):
+    """Inputs of the reference's own shader logic (oracle/_ref: a mechanical
+    C++ translation of lbvh.wgsl + barnes_hut.wgsl, independent stages on all
+    host threads) for a workload: its bodies from the oracle's generator (one
+    PCG32 stream per body: the workload's distribution and size), its theta
+    and dt.  The reference knows only its own softening, eps = epsMult
     sqrt(G max(m1, m2) dt); epsMult is set so that eps equals the workload's
-    Plummer eps at the median body mass.  Up to a million bodies every step
-    runs whole; above, the walk (velocity step) runs on every k-th sorted
-    slot and its time is scaled by k, the other stages run whole."""
+    Plummer eps at the median body mass."""
     orc = _oracle()
-    if not orc.ref_available():
-        return None
     op = wp["oracle"]
     n, G, dt = wp["n"], op["G"], op["dt"]
     mass, pos, vel, _ = orc.generate_per_body(wp["scenario"], n, 1, G)
     m_med = float(np.median(mass))
     eps_mult = float(op["plummer_eps"] / np.sqrt(G * m_med * dt))
-    stride = 1 if n <= 1_000_000 else max(1, n // 250_000)
-    kw = dict(G=G, dt=dt, eps_mult=eps_mult, theta=op["theta"], walk_stride=stride)
-    one = orc.ref_run_timed(mass, pos, vel, steps=1, **kw)  # warm-up and size the sample
-    per_step = sum(one.values()) + one["vel_step"] * (stride - 1)
-    steps = int(max(1, min(50, seconds_budget / max(per_step, 1e-3))))
-    st = orc.ref_run_timed(mass, pos, vel, steps=steps, **kw)
-    el = st["morton"] + st["sort"] + st["build_fill"] + stride * st["vel_step"] + st["pos_step"]
-    threads = orc.ref_threads()
+    kw = dict(G=G, dt=dt, eps_mult=eps_mult, theta=op["theta"])
+    return orc, n, (mass, pos, vel), kw
+
+
+def _ref_seconds(st: dict, stride: int) -> float:
+    """Host seconds of timed reference steps, the sampled walk scaled."""
+    return st["morton"] + st["sort"] + st["build_fill"] + stride * st["vel_step"] + st["pos_step"]
+
+
+def _ref_sample(what: str, n: int, stride: int, eps_mult: float, threads: int) -> str:
     walk = ("the whole walk" if stride == 1 else
             f"the walk timed on every {stride}th sorted slot and scaled by {stride}")
-    return {"value": n * steps / el, "unit": "body-steps/s", "cores": threads, "kind": "reference",
+    return (f"{what} of the {n}-body workload, {walk} (reference WGSL logic translated to C++: "
+            f"the reference's fixed 2000-unit Morton domain (lbvh.wgsl:49-57), so the workload's "
+            f"bodies share few grid cells; per-body monopole walk; epsMult {eps_mult:.1f}; "
+            f"{threads} OpenMP threads; fill serial; bodies from the oracle's generator)")
+
+
+def reference_baseline(wp: dict, seconds_budget=20.0):
+    """cpu_baseline leg: the reference's own shader logic (_ref_setup) for
+    about `seconds_budget` of whole steps.  Up to a million bodies every step
+    runs whole; above, the walk (velocity step) runs on every k-th sorted
+    slot and its time is scaled by k, the other stages run whole."""
+    orc = _oracle()
+    if not orc.ref_available():
+        return None
+    orc, n, bodies, kw = _ref_setup(wp)
+    stride = 1 if n <= 1_000_000 else max(1, n // 250_000)
+    one = orc.ref_run_timed(*bodies, steps=1, walk_stride=stride, **kw)  # warm-up, sizes the sample
+    per_step = _ref_seconds(one, 1) + one["vel_step"] * (stride - 1)
+    steps = int(max(1, min(50, seconds_budget / max(per_step, 1e-3))))
+    st = orc.ref_run_timed(*bodies, steps=steps, walk_stride=stride, **kw)
+    threads = orc.ref_threads()
+    return {"value": n * steps / _ref_seconds(st, stride), "unit": "body-steps/s", "cores": threads,
+            "kind": "reference", "stages_s_per_step": {k: v / steps for k, v in st.items()},
+            "walk_stride": stride,
+            "sample": _ref_sample(f"{steps} steps", n, stride, kw["eps_mult"], threads)}
+
+
+def reference_arm(wp: dict, steps: int, warmup: int, seconds_total=180.0):
+    """--impl reference: `warmup` untimed steps, then exactly `steps` timed
+    steps of the reference's own shader logic (_ref_setup) on the workload,
+    each a bounded sample so that the whole run takes about `seconds_total`
+    of host time.  A probe step (the walk on every k-th sorted slot above a
+    million bodies) measures the stages; a step runs whole when it fits its
+    share of the time, else its walk runs on every k-th sorted slot, k the
+    smallest that fits, and the walk's time is scaled by k.  Falls back to
+    the oracle port when oracle/_ref was not built."""
+    orc = _oracle()
+    steps = max(1, int(steps))
+    warmup = max(0, int(warmup))
+    if not orc.ref_available():
+        return port_arm(wp, steps, warmup)
+    orc, n, bodies, kw = _ref_setup(wp)
+    probe = 1 if n <= 1_000_000 else max(1, n // 250_000)
+    one = orc.ref_run_timed(*bodies, steps=1, walk_stride=probe, **kw)
+    walk = one["vel_step"] * probe  # whole-walk seconds of one step
+    other = _ref_seconds(one, probe) - walk
+    share = seconds_total / (steps + warmup)
+    avail = max(share - other, 0.05)
+    stride = 1 if walk <= avail else min(n, -(-int(walk * 1e6) // max(int(avail * 1e6), 1)))
+    if warmup:
+        orc.ref_run_timed(*bodies, steps=warmup, walk_stride=stride, **kw)
+    st = orc.ref_run_timed(*bodies, steps=steps, walk_stride=stride, **kw)
+    threads = orc.ref_threads()
+    return {"value": n * steps / _ref_seconds(st, stride), "unit": "body-steps/s",
+            "cores": threads, "kind": "reference",
             "stages_s_per_step": {k: v / steps for k, v in st.items()}, "walk_stride": stride,
-            "sample": f"{steps} steps of the {n}-body workload, {walk} (reference WGSL logic "
-                      f"translated to C++: the reference's fixed 2000-unit Morton domain "
-                      f"(lbvh.wgsl:49-57), so the workload's bodies share few grid cells; "
-                      f"per-body monopole walk; epsMult {eps_mult:.1f}; {threads} OpenMP threads; "
-                      f"fill serial; bodies from the oracle's generator)"}
+            "sample": _ref_sample(f"{warmup} untimed then {steps} timed steps", n, stride,
+                                  kw["eps_mult"], threads)}
+
+
+def port_arm(wp: dict, steps: int, warmup: int):
+    """The oracle port (C restatement, OpenMP) in place of oracle/_ref:
+    `warmup` untimed steps, then `steps` timed whole steps."""
+    orc = _oracle()
+    op = wp["oracle"]
+    n = wp["n"]
+    mass, pos, vel, _ = orc.generate_per_body(wp["scenario"], n, 1, op["G"])
+    st = orc.State(orc.params(**op), mass, pos, vel)
+    threads = orc.load().orc_max_threads()
+    st.step(1)  # includes the initial force evaluation of the leapfrog
+    if warmup:
+        st.step(warmup)
+    t0 = time.perf_counter()
+    st.step(steps)
+    el = time.perf_counter() - t0
+    return {"value": n * steps / el, "unit": "body-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{warmup} untimed then {steps} timed whole steps of the {n}-body workload "
+                      f"(oracle C restatement, same algorithm as the engine: {op['walk']} walk, "
+                      f"{threads} OpenMP threads)"}
 
 
 def cpu_baseline(wp: dict, seconds_budget=20.0):
@@ -666,6 +743,24 @@ def port_baseline(wp: dict, seconds_budget=20.0):
                       f"{threads} OpenMP threads)"}
 
 
+# ---------------------------------------------------------------- both arms
+
+def run_config(args, n, theta, plummer_eps, dt, integrator, world):
+    """The line's `config`: the workload both arms run, how a run with
+    `world` ranks divides it, and how timed steps treat the caches.  Both
+    arms build it here from the same values (the workload table the test
+    suite checks against the package's), so the two lines carry one config;
+    each implementation's own choices are reported beside it."""
+    sharded = args.shard or (world > 1 and not args.replicas)
+    return {"workload": args.workload, "bodies": n, "theta": theta,
+            "softening": f"plummer {plummer_eps}", "dt": dt, "integrator": integrator,
+            "parallelism": (f"shard{world} (sorted-slot ranges, one all-gather of "
+                            f"16 B/body per step)" if sharded else
+                            f"replicas{world}" if world > 1 else "single"),
+            "l2": ("device timing: L2 flushed between timed steps (256 MB write, outside the "
+                   "events); host timing: no device cache involved")}
+
+
 # ---------------------------------------------------------------- reference arm
 
 def run_reference(args):
@@ -675,15 +770,16 @@ def run_reference(args):
     if rank != 0:
         return 0
     wp = REF_WORKLOADS[args.workload]
-    # Each step is a bounded sample of the workload, sized so the whole
-    # --steps K --warmup W run stays within a few minutes.
-    budget = max(10.0, 120.0 / max(args.steps + args.warmup, 1))
-    cb = cpu_baseline(wp, seconds_budget=budget)
+    op = wp["oracle"]
+    # W untimed steps, then K timed ones, each a bounded sample of the
+    # workload so the whole run stays within a few minutes.
+    cb = reference_arm(wp, args.steps, args.warmup)
     line = {"impl": "reference", "metric": "body-steps/s", "value": cb["value"],
             "unit": "body-steps/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG32)",
-            "config": {"workload": args.workload, "bodies": wp["n"]},
+            "config": run_config(args, wp["n"], op["theta"], op["plummer_eps"], op["dt"],
+                                 op["integrator"], int(os.environ.get("WORLD_SIZE", "1"))),
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "body-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -830,17 +926,13 @@ def run_own(args):
             "higher_is_better": True, "scaling": "strong" if sharded is not None else "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded PCG32 colliding exponential disks)",
-            "config": {"workload": args.workload, "bodies": n, "theta": cfg.bhTheta,
-                       "softening": f"plummer {cfg.plummerEps}", "dt": cfg.deltaTime,
-                       "integrator": cfg.integrator, "morton_bits": cfg.mortonBits,
+            "config": run_config(args, n, cfg.bhTheta, cfg.plummerEps, cfg.deltaTime,
+                                 cfg.integrator, world),
+            "engine": {"morton_bits": cfg.mortonBits,
                        "walk": f"{cfg.walk}, multipole order {cfg.multipole}",
                        "bodies_per_lane": cfg.bodiesPerLane, "leaf_size": cfg.leafSize,
                        "walk_block": cfg.walkBlock, "far_alpha": cfg.farAlpha,
-                       "autotuned": tune is not None, "shape_pinned": bool(args.walk_shape),
-                       "parallelism": (f"shard{world} (sorted-slot ranges, one all-gather of "
-                                       f"16 B/body per step)" if sharded is not None else
-                                       f"replicas{world}" if world > 1 else "single"),
-                       "l2": "flushed between timed steps (256 MB write, outside the events)"},
+                       "autotuned": tune is not None, "shape_pinned": bool(args.walk_shape)},
             "roofline": roofline,
             "stages_ms": stages,
             "stream_stages": stream_rooflines(stages, n, 8 if cfg.mortonBits == 64 else 4, hbm),

@@ -54,6 +54,42 @@ def test_reference_arm_runs_without_the_engine(orc):
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["cpu_baseline"]["kind"] in ("reference", "port")
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+    # W untimed, then exactly K timed steps; the own arm's config
+    assert line["steps"] == 3 and line["warmup"] == 3
+    assert "3 untimed then 3 timed" in line["cpu_baseline"]["sample"]
+    assert line["config"] == _own_config(_bench(), "uniform-disk-16k", 1, [])
+
+
+def _own_config(bench, name, world, flags):
+    """The config the own arm prints for a workload (its values from the
+    package's WORKLOADS, as run_own takes them)."""
+    argv, sys.argv = sys.argv, ["bench.py", "--workload", name, *flags]
+    try:
+        args = bench.parse()
+    finally:
+        sys.argv = argv
+    import importlib
+    wl = importlib.import_module("webgpu-fluid-sim_b200").WORKLOADS[name]
+    cfg = wl["config"]
+    return bench.run_config(args, wl["n"], cfg.bhTheta, cfg.plummerEps, cfg.deltaTime,
+                            cfg.integrator, world)
+
+
+@pytest.mark.parametrize("world,flags", [(1, []), (2, []), (2, ["--replicas"]), (1, ["--shard"])])
+def test_both_arms_print_one_config(bh, world, flags):
+    bench = _bench()
+    for name, wp in bench.REF_WORKLOADS.items():
+        own = _own_config(bench, name, world, flags)
+        argv, sys.argv = sys.argv, ["bench.py", "--impl", "reference", "--workload", name, *flags]
+        try:
+            args = bench.parse()
+        finally:
+            sys.argv = argv
+        op = wp["oracle"]
+        ref = bench.run_config(args, wp["n"], op["theta"], op["plummer_eps"], op["dt"],
+                               op["integrator"], world)
+        assert own == ref, name
+        assert own["workload"] == name and own["bodies"] == wp["n"]
 
 
 def test_walk_roofline_flop_convention():
