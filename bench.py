@@ -761,6 +761,10 @@ def run_config(args, n, theta, plummer_eps, dt, integrator, world):
                    "events); host timing: no device cache involved")}
 
 
+def run_data(scenario: str) -> str:
+    return f"synthetic (seeded PCG32 scenario {scenario!r}; no dataset exists for this path)"
+
+
 # ---------------------------------------------------------------- reference arm
 
 def run_reference(args):
@@ -777,7 +781,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": "body-steps/s", "value": cb["value"],
             "unit": "body-steps/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG32)",
+            "vs_baseline": None, "dtype": "f32", "data": run_data(wp["scenario"]),
             "config": run_config(args, wp["n"], op["theta"], op["plummer_eps"], op["dt"],
                                  op["integrator"], int(os.environ.get("WORLD_SIZE", "1"))),
             "cpu_baseline": cb,
@@ -925,7 +929,7 @@ def run_own(args):
             "steps": K, "warmup": args.warmup, "ms_per_step": step_ms_max / K,
             "higher_is_better": True, "scaling": "strong" if sharded is not None else "weak",
             "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded PCG32 colliding exponential disks)",
+            "data": run_data(wl["scenario"]),
             "config": run_config(args, n, cfg.bhTheta, cfg.plummerEps, cfg.deltaTime,
                                  cfg.integrator, world),
             "engine": {"morton_bits": cfg.mortonBits,

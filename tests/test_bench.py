@@ -58,6 +58,7 @@ def test_reference_arm_runs_without_the_engine(orc):
     assert line["steps"] == 3 and line["warmup"] == 3
     assert "3 untimed then 3 timed" in line["cpu_baseline"]["sample"]
     assert line["config"] == _own_config(_bench(), "uniform-disk-16k", 1, [])
+    assert "uniform-disk-kepler" in line["data"]
 
 
 def _own_config(bench, name, world, flags):
