@@ -104,3 +104,12 @@ def test_walk_roofline_flop_convention():
     assert r["achieved"] == pytest.approx(r["flops_per_step"] / 1e-3 / 1e12)
     s = bench.stream_rooflines({"sort": 1.0}, 1_000_000, 8, 6000.0)
     assert s["sort"]["bytes_per_body"] == 20 + 7 * 24
+
+
+def test_reference_arm_port_fallback(orc):
+    # Without oracle/_ref the arm times the oracle port, with the same
+    # warm-up / timed structure.
+    bench = _bench()
+    cb = bench.port_arm(bench.REF_WORKLOADS["uniform-disk-16k"], 2, 1)
+    assert cb["kind"] == "port" and cb["value"] > 0 and cb["cores"] >= 1
+    assert "1 untimed then 2 timed whole steps of the 16384-body workload" in cb["sample"]
