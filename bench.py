@@ -49,6 +49,7 @@ import argparse
 import dataclasses
 import importlib
 import json
+import math
 import os
 import subprocess
 import sys
@@ -682,7 +683,7 @@ def reference_arm(wp: dict, steps: int, warmup: int, seconds_total=180.0):
     other = _ref_seconds(one, probe) - walk
     share = seconds_total / (steps + warmup)
     avail = max(share - other, 0.05)
-    stride = 1 if walk <= avail else min(n, -(-int(walk * 1e6) // max(int(avail * 1e6), 1)))
+    stride = 1 if walk <= avail else min(n, math.ceil(walk / avail))
     if warmup:
         orc.ref_run_timed(*bodies, steps=warmup, walk_stride=stride, **kw)
     st = orc.ref_run_timed(*bodies, steps=steps, walk_stride=stride, **kw)
