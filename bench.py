@@ -632,9 +632,14 @@ def _ref_seconds(st: dict, stride: int) -> float:
     return st["morton"] + st["sort"] + st["build_fill"] + stride * st["vel_step"] + st["pos_step"]
 
 
+def _ordinal(k: int) -> str:
+    suffix = "th" if 10 <= k % 100 <= 20 else {1: "st", 2: "nd", 3: "rd"}.get(k % 10, "th")
+    return f"{k}{suffix}"
+
+
 def _ref_sample(what: str, n: int, stride: int, eps_mult: float, threads: int) -> str:
     walk = ("the whole walk" if stride == 1 else
-            f"the walk timed on every {stride}th sorted slot and scaled by {stride}")
+            f"the walk timed on every {_ordinal(stride)} sorted slot and scaled by {stride}")
     return (f"{what} of the {n}-body workload, {walk} (reference WGSL logic translated to C++: "
             f"the reference's fixed 2000-unit Morton domain (lbvh.wgsl:49-57), so the workload's "
             f"bodies share few grid cells; per-body monopole walk; epsMult {eps_mult:.1f}; "

@@ -113,3 +113,28 @@ def test_reference_arm_port_fallback(orc):
     cb = bench.port_arm(bench.REF_WORKLOADS["uniform-disk-16k"], 2, 1)
     assert cb["kind"] == "port" and cb["value"] > 0 and cb["cores"] >= 1
     assert "1 untimed then 2 timed whole steps of the 16384-body workload" in cb["sample"]
+
+
+def test_reference_arm_samples_the_walk_when_a_step_does_not_fit(orc, monkeypatch):
+    # A whole step (8 s of walk) longer than its share of the run (30 s over
+    # 6 steps): the walk runs on every 2nd sorted slot and its time is scaled
+    # by 2; W untimed and K timed steps as asked.
+    bench = _bench()
+    calls = []
+
+    def fake(mass, pos, vel, steps=1, walk_stride=1, **kw):
+        calls.append((steps, walk_stride))
+        return {"morton": 0.01 * steps, "sort": 0.01 * steps, "build_fill": 0.01 * steps,
+                "vel_step": 8.0 * steps / walk_stride, "pos_step": 0.01 * steps}
+
+    monkeypatch.setattr(orc, "ref_run_timed", fake)
+    monkeypatch.setattr(orc, "ref_available", lambda: True)
+    monkeypatch.setattr(orc, "ref_threads", lambda: 4)
+    wp = bench.REF_WORKLOADS["uniform-disk-16k"]
+    cb = bench.reference_arm(wp, 5, 1, seconds_total=30.0)
+    assert calls == [(1, 1), (1, 2), (5, 2)]
+    assert cb["walk_stride"] == 2 and cb["kind"] == "reference"
+    assert cb["value"] == pytest.approx(16384 * 5 / (0.04 * 5 + 2 * 8.0 * 5 / 2))
+    assert "every 2nd sorted slot and scaled by 2" in cb["sample"]
+    assert [bench._ordinal(k) for k in (1, 2, 3, 4, 11, 12, 13, 21, 67, 112)] == \
+        ["1st", "2nd", "3rd", "4th", "11th", "12th", "13th", "21st", "67th", "112th"]
